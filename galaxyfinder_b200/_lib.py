@@ -1,0 +1,150 @@
+"""ctypes binding of libgf.so (the C ABI declared in include/gf.h).
+
+The library is built in-tree by ``galaxyfinder_b200.build`` and loaded from
+this package directory.  There is no fallback: if the library is missing or
+fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libgf.so"
+
+# status codes (gf.h)
+GF_OK, GF_EINVAL, GF_ENOMEM, GF_EDEVICE, GF_ETIMEOUT, GF_ERANGE, GF_ENOTIMPL = range(7)
+
+# particle types (NewGalFinder/tree.h:47-48)
+TYPE_STAR, TYPE_DM, TYPE_GAS, TYPE_SINK, TYPE_ALL = 1, 2, 3, 4, 5
+
+# SimpleBasicParticleType, NewGalFinder/tree.h:155-162 (88 bytes)
+BP_DTYPE = np.dtype([
+    ("type", "<u4"), ("_pad0", "<u4"), ("mass", "<f8"), ("x", "<f8"), ("y", "<f8"),
+    ("z", "<f8"), ("vx", "<f8"), ("vy", "<f8"), ("vz", "<f8"), ("link02", "<f8"),
+    ("indx", "<i4"), ("_pad1", "<i4"), ("bp", "<u8"),
+])
+assert BP_DTYPE.itemsize == 88
+
+# Vector3d, NewGalFinder/subhaloden.mod6.c:70-72
+VEC3_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8")])
+
+# gf_mesh_desc (gf.h), 64 bytes
+MESH_DTYPE = np.dtype([
+    ("off", "<i8"), ("nx", "<i4"), ("ny", "<i4"), ("nz", "<i4"), ("ptype", "<i4"),
+    ("xmin", "<f8"), ("ymin", "<f8"), ("zmin", "<f8"), ("cellsize", "<f8"), ("rg", "<f8"),
+])
+assert MESH_DTYPE.itemsize == 64
+
+MESH_REFERENCE, MESH_FIXED, MESH_POW2 = 0, 1, 2
+
+
+class MeshRule(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32), ("nfixed", ctypes.c_int32), ("nmin", ctypes.c_int32),
+        ("nmax", ctypes.c_int32), ("nbuff", ctypes.c_int32), ("ptype", ctypes.c_int32),
+        ("rg_in_cells", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("cell", ctypes.c_double), ("rg", ctypes.c_double),
+    ]
+
+
+class Batch(ctypes.Structure):
+    _fields_ = [
+        ("nhalo", ctypes.c_int32), ("nparticle", ctypes.c_int64), ("pstart", ctypes.c_void_p),
+        ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
+        ("mass", ctypes.c_void_p), ("type", ctypes.c_void_p),
+    ]
+
+
+class Physics(ctypes.Structure):
+    _fields_ = [
+        ("amax", ctypes.c_float), ("a", ctypes.c_float), ("omep", ctypes.c_float),
+        ("omeplam", ctypes.c_float), ("hubble", ctypes.c_float),
+        ("potentfact", ctypes.c_double), ("r1kineticfact", ctypes.c_double),
+        ("r2kineticfact", ctypes.c_double),
+    ]
+
+
+class GFError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"libgf status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+_VP, _I32, _I64, _F, _D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+_INT = ctypes.c_int
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "gf_status_string": (ctypes.c_char_p, [_INT]),
+    "gf_last_status": (_INT, []),
+    "gf_last_error": (ctypes.c_char_p, []),
+    "gf_set_device": (_INT, [_INT]),
+    "gf_kernel_launch_count": (ctypes.c_uint64, []),
+    "gf_set_cosmology": (_INT, [_F, _F, _F, _F, _F]),
+    "gf_get_physics": (_INT, [ctypes.POINTER(Physics)]),
+    "gf_bg_potent": (_D, [_D]),
+    "assign_density_TSC": (None, [_VP, _INT, _VP, _INT, _INT, _INT, _D, _D, _D, _D, _INT]),
+    "findDen": (None, [_VP, _INT, _VP, _D, _D, _D, _D, _VP, _INT, _INT, _INT]),
+    "gaussian_Smoothing": (None, [_VP, _INT, _INT, _INT, _D, _F]),
+    "findsphdensity": (None, [_VP, _INT, _VP, _INT, _VP]),
+    "Self_Halo_Potent": (None, [_INT, _VP, _VP, _VP]),
+    "External_Halo_Potent": (None, [_INT, _VP, _VP, _VP, _INT, _VP, _VP]),
+    "i_potent_spline": (None, []),
+    "gf_ctx_create": (_INT, [ctypes.POINTER(_VP), _INT, _VP]),
+    "gf_ctx_destroy": (_INT, [_VP]),
+    "gf_ctx_set_stream": (_INT, [_VP, _VP]),
+    "gf_plan_meshes": (_INT, [_I32, _VP, ctypes.POINTER(MeshRule), _VP, ctypes.POINTER(_I64)]),
+    "gf_mesh_stage": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP, _VP, _INT]),
+    "gf_tsc_deposit": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP]),
+    "gf_gaussian_smooth": (_INT, [_VP, _I32, _VP, _VP, _VP]),
+    "gf_find_den": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP]),
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libgf.so (once).  Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(
+                f"{LIB_PATH} is not built; run `python -m galaxyfinder_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != GF_OK:
+        msg = lib().gf_last_error().decode(errors="replace")
+        raise GFError(status, msg or lib().gf_status_string(status).decode())
+
+
+def check_last() -> None:
+    """Raises if the last drop-in (void) call on this thread failed."""
+    check(lib().gf_last_status())
+
+
+def ptr(a) -> int:
+    """Address of a numpy array or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)
+
+
+def default_device() -> int:
+    return int(os.environ.get("GF_DEVICE", "0"))

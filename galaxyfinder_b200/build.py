@@ -1,0 +1,67 @@
+"""Builds libgf.so (the CUDA kernels + C ABI) in-tree for sm_100a.
+
+    python -m galaxyfinder_b200.build          # incremental
+    python -m galaxyfinder_b200.build --force  # rebuild everything
+
+Each translation unit under csrc/ is compiled by nvcc for
+``arch=compute_100a,code=sm_100a`` with ``-lineinfo``; the objects are
+linked into ``galaxyfinder_b200/libgf.so``.  ``gf_tsc.cu`` and ``gf_knn.cu``
+are compiled with ``--fmad=false`` because their results must reproduce the
+reference's separately rounded float/double arithmetic bit for bit.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libgf.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NOFMAD = {"gf_tsc.cu", "gf_knn.cu"}
+
+
+def nvcc() -> str:
+    cand = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    return cand
+
+
+def _flags(name: str) -> list[str]:
+    f = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-O2",
+         "-I", str(ROOT / "include"), "-I", str(CSRC), "--expt-relaxed-constexpr"]
+    if name in NOFMAD:
+        f.append("--fmad=false")
+    return f
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    sources = sorted(CSRC.glob("*.cu"))
+    headers = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
+    newest_header = max((h.stat().st_mtime for h in headers), default=0.0)
+    objs = []
+    for src in sources:
+        obj = BUILD / (src.stem + ".o")
+        objs.append(obj)
+        stale = force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header)
+        if not stale:
+            continue
+        cmd = [nvcc(), *_flags(src.name), "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [nvcc(), "-shared", *ARCH, "-o", str(LIB), *map(str, objs), "-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

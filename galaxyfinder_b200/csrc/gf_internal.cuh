@@ -1,0 +1,130 @@
+// Internal declarations shared by the libgf CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gf.h"
+
+namespace gf {
+
+// ---------------------------------------------------------------- status
+void set_status(int status, const char *fmt, ...);
+void clear_status();
+int last_status();
+
+// Counts every kernel launch issued through libgf.
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+#define GF_CUDA_TRY(call)                                                                     \
+    do {                                                                                      \
+        cudaError_t _e = (call);                                                              \
+        if (_e != cudaSuccess) {                                                              \
+            ::gf::set_status(GF_EDEVICE, "%s:%d %s: %s", __FILE__, __LINE__, #call,          \
+                             cudaGetErrorString(_e));                                         \
+            return GF_EDEVICE;                                                                \
+        }                                                                                     \
+    } while (0)
+
+#define GF_LAUNCH_CHECK()                                                                     \
+    do {                                                                                      \
+        ::gf::count_launch();                                                                 \
+        cudaError_t _e = cudaGetLastError();                                                  \
+        if (_e != cudaSuccess) {                                                              \
+            ::gf::set_status(GF_EDEVICE, "%s:%d launch failed: %s", __FILE__, __LINE__,      \
+                             cudaGetErrorString(_e));                                         \
+            return GF_EDEVICE;                                                                \
+        }                                                                                     \
+    } while (0)
+
+#define GF_TRY(expr)                                                                          \
+    do {                                                                                      \
+        int _s = (expr);                                                                      \
+        if (_s != GF_OK) return _s;                                                           \
+    } while (0)
+
+// Device error word bits (set by kernels with atomicOr, read back by the host).
+enum : int {
+    GF_ERRBIT_RANGE = 1,      // a particle's TSC stencil left its mesh
+    GF_ERRBIT_TREE = 2,       // tree build ran out of node capacity
+    GF_ERRBIT_KNN = 4,        // a kNN query found fewer than k neighbours
+    GF_ERRBIT_WALK = 8,       // a tree walk exceeded its step bound
+};
+
+// ---------------------------------------------------------------- workspace
+// Grow-only device allocation owned by a context.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t need);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+struct HostPinned {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t need);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+}  // namespace gf
+
+struct gf_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int *d_err = nullptr;  // device error word
+    // scratch buffers, named by use
+    gf::DevBuf hid, mesh, smooth_tiles, smooth_tables, particles, tmp[8];
+    gf::DevBuf tree[16];
+    gf::HostPinned pin[4];
+    std::mutex lock;
+};
+
+namespace gf {
+
+// The context used by the drop-in (reference-signature) entry points.
+gf_ctx *default_ctx();
+
+// Reads and clears the device error word; maps set bits to a status.
+int check_device_errors(gf_ctx *ctx);
+
+// Fill hid[i] = halo index of particle i from pstart (device).
+int compute_hid(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart, int32_t *hid);
+
+// Mesh helpers implemented in gf_smooth.cu / gf_tsc.cu.
+int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                       const double *mass, const int32_t *type, const int32_t *hid,
+                       const gf_mesh_desc *mesh, float *den, double volfact);
+int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                    const int32_t *hid, const gf_mesh_desc *mesh, const float *den, float *densph);
+int launch_scale(gf_ctx *ctx, float *den, int64_t ncells, double factor);
+int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
+                  const gf_mesh_desc *mesh_dev, float *den);
+
+inline int64_t mesh_cells(const gf_mesh_desc &m) {
+    return (int64_t)(2 * (m.nx / 2 + 1)) * m.ny * m.nz;
+}
+
+// Halo frames (per axis: min and periodic-shift flag) and recentred extents.
+int halo_frames(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, double box,
+                std::vector<double> &frame_host, std::vector<double> &extent_host);
+// FP64 recentring (Dump2BP) -> double SoA + float4 (x, y, z, mass).
+int recentre(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, const double *frame_dev,
+             double box, double *xr, double *yr, double *zr, float4 *pos);
+gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r);
+
+// volfact of tsc_omp2.c:188 for the reference cell size 0.004 cMpc/h.
+double tsc_volfact();
+// True when volfact is folded into the deposit weights (exact power of two).
+bool volfact_folds(double v);
+
+}  // namespace gf

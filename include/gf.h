@@ -1,0 +1,171 @@
+/* libgf — B200-native density-and-potential stage of the PGalF galaxy finder
+ * (NewGalFinder's per-halo kNN/SPH density, TSC mass assignment, FFT Gaussian
+ * smoothing, mesh-density interpolation and Barnes-Hut potential).
+ *
+ * Two layers, both plain C ABI (no C++ or torch types in any signature):
+ *
+ *  1. Drop-in entry points with the reference's exact C signatures.  A
+ *     reference build links libgf ahead of its own objects (or weakens its own
+ *     definitions) and the calls from subhalo_den()/lagFindStellarCore() land
+ *     here.  They take the reference's host buffers, copy them to the GPU,
+ *     run the kernels and copy results back before returning, so no host
+ *     pointer is kept across calls (the reference's Memory2.c arena may move
+ *     blocks between calls, Memory2.c:173-195).  Errors never call exit():
+ *     the status is kept in gf_last_status()/gf_last_error().
+ *
+ *  2. The native batched API (gf_*): device pointers, many halos per call,
+ *     stream-ordered, returning an int status.
+ *
+ * Status codes: */
+#ifndef GF_H
+#define GF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "gf_ref_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GF_OK 0
+#define GF_EINVAL 1    /* bad argument (size, pointer, mesh too small for the particles) */
+#define GF_ENOMEM 2    /* device or host allocation failed */
+#define GF_EDEVICE 3   /* CUDA error or no usable device */
+#define GF_ETIMEOUT 4  /* a device-side bounded wait gave up */
+#define GF_ERANGE 5    /* a particle fell outside its mesh (the reference would write out of bounds) */
+#define GF_ENOTIMPL 6
+
+const char *gf_status_string(int status);
+/* Status and message of the most recent call made by this host thread. */
+int gf_last_status(void);
+const char *gf_last_error(void);
+/* Select the CUDA device the drop-in entry points use (default: 0, or the
+ * GF_DEVICE environment variable).  Returns a status. */
+int gf_set_device(int device);
+/* Number of kernels this process has launched through libgf (for tests that
+ * must prove the GPU path ran). */
+uint64_t gf_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------------
+ * Physics constants used by the potential drivers.  They are the values the
+ * reference computes in physical_parameters() (NewGalFinder/gfind.c:842-890)
+ * and reads as globals (potentfact, r1kineticfact, r2kineticfact, amax, a,
+ * omep).  Defaults: amax = a = 1, omep = 0.3, omeplam = 0.7, hubble = 70.
+ * ---------------------------------------------------------------------- */
+typedef struct gf_physics {
+    float amax, a, omep, omeplam, hubble;
+    double potentfact, r1kineticfact, r2kineticfact;
+} gf_physics;
+
+/* Recompute potentfact/r1kineticfact/r2kineticfact from the cosmology in
+ * `ph` (gfind.c:842-890) and store it for the drop-in potential drivers. */
+int gf_set_cosmology(float amax, float a, float omep, float omeplam, float hubble);
+int gf_get_physics(gf_physics *out);
+/* NFW background potential of a halo of mass mvir (subhaloden.mod6.c:1093). */
+double gf_bg_potent(double mvir);
+
+/* ------------------------------------------------------------------------
+ * Drop-in entry points (reference signatures; host pointers; synchronous).
+ * ---------------------------------------------------------------------- */
+
+/* NewGalFinder/tsc_omp2.c:166.  den holds mx*ny*nz floats, mx = 2(nx/2+1). */
+void assign_density_TSC(SimpleBasicParticleType *bp, int np, float *den, int nx, int ny, int nz,
+                        double Xmin, double Ymin, double Zmin, double cellsize, int ptype);
+/* NewGalFinder/tsc_omp2.c:40 */
+void findDen(SimpleBasicParticleType *bp, int np, float *densph, double xmin, double ymin,
+             double zmin, double cellsize, float *den, int nx, int ny, int nz);
+/* NewGalFinder/gsmooth.c:14.  In place on mx*ny*nz floats. */
+void gaussian_Smoothing(float *denGrid, int nx, int ny, int nz, double cellsize, float RG);
+/* NewGalFinder/nnost.c:560.  nearindex holds np*Numnear indices into bp. */
+void findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, int Numnear,
+                    float *densph);
+/* NewGalFinder/subhaloden.mod6.c:1477 */
+void Self_Halo_Potent(int np, Vector3d *r, float *mass, float *penergy);
+/* NewGalFinder/subhaloden.mod6.c:1537 */
+void External_Halo_Potent(int nend, Vector3d *r, float *mass, float *penergy, int snp,
+                          Vector3d *sr, float *smass);
+/* NewGalFinder/force_spline.mod3.c:81.  The GPU potential evaluates the
+ * kernel -1/r and its quadrupole terms exactly, so no table is built; the
+ * call only initialises the device. */
+void i_potent_spline(void);
+
+/* ------------------------------------------------------------------------
+ * Native batched API.
+ * ---------------------------------------------------------------------- */
+typedef struct gf_ctx gf_ctx;
+
+/* stream: a cudaStream_t (NULL = legacy default stream). */
+int gf_ctx_create(gf_ctx **ctx, int device, void *stream);
+int gf_ctx_destroy(gf_ctx *ctx);
+int gf_ctx_set_stream(gf_ctx *ctx, void *stream);
+
+/* Per-halo mesh description (device array, one entry per halo).  The mesh of
+ * halo h occupies den[off, off + mx*ny*nz) with mx = 2(nx/2+1), laid out as
+ * den[i + mx*(j + ny*k)] (tsc_omp2.c:16).  Positions handed to the mesh
+ * kernels are in the same frame as (xmin, ymin, zmin). */
+typedef struct gf_mesh_desc {
+    int64_t off;
+    int32_t nx, ny, nz;
+    int32_t ptype;          /* TSC particle filter; GF_TYPE_ALL = every particle */
+    double xmin, ymin, zmin;
+    double cellsize;
+    double rg;              /* Gaussian smoothing length (same unit as cellsize) */
+} gf_mesh_desc;
+
+/* Particle batch in device memory: halos are contiguous ranges
+ * [pstart[h], pstart[h+1]) of the particle arrays. */
+typedef struct gf_batch {
+    int32_t nhalo;
+    int64_t nparticle;
+    const int64_t *pstart;   /* device, nhalo+1 */
+    const double *x, *y, *z; /* device, FP64 positions (cMpc/h) */
+    const double *mass;      /* device, FP64 (Msun/h) */
+    const int32_t *type;     /* device, may be NULL (all GF_TYPE_DM) */
+} gf_batch;
+
+/* Per-halo mesh sizing rules (the mesh of a halo is planned from its
+ * recentred extent; the origin is nbuff/2 cells below the halo minimum and
+ * the upper bound is padded by 1e-4 of the extent, nnost.c:1040-1056). */
+#define GF_MESH_REFERENCE 0 /* n = extent/cell + nbuff per axis (nnost.c:1053-1055) */
+#define GF_MESH_FIXED 1     /* cubic n = nfixed; cell = max extent / (n - nbuff) */
+#define GF_MESH_POW2 2      /* cubic n = clamp(next_pow2(extent/cell + nbuff), nmin, nmax);
+                               cell grows beyond `cell` when the halo needs more than nmax */
+typedef struct gf_mesh_rule {
+    int32_t mode;
+    int32_t nfixed, nmin, nmax;
+    int32_t nbuff;          /* NCELLBUFF (params.h:115), 10 */
+    int32_t ptype;          /* TSC particle filter */
+    int32_t rg_in_cells;    /* 1: rg is in units of the planned cell size */
+    int32_t reserved;
+    double cell;            /* TSC_CELL_SIZE (params.h:92), 0.004 cMpc/h */
+    double rg;              /* Gaussian_Smoothing_Length (params.h:104), 0.008 cMpc/h */
+} gf_mesh_rule;
+
+/* Plans one mesh per halo from extent[3*h + axis] (recentred extents,
+ * cMpc/h); writes desc[h] with consecutive, 256-byte aligned offsets and
+ * returns the total float count in *total_cells.  Host-only. */
+int gf_plan_meshes(int32_t nhalo, const double *extent, const gf_mesh_rule *rule,
+                   gf_mesh_desc *desc, int64_t *total_cells);
+
+/* Mesh stage on a batch whose meshes are already described: zero + TSC
+ * deposit (tsc_omp2.c:166), Gaussian smoothing (gsmooth.c:14) and the
+ * interpolation back to every particle (tsc_omp2.c:40).  den must hold the
+ * sum of all meshes; densph one float per particle.  If smoothed_only is 0
+ * the raw deposit is left in den and densph is not written. */
+int gf_mesh_stage(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh_dev,
+                  const gf_mesh_desc *mesh_host, float *den, float *densph, int smooth);
+
+/* Individual batched mesh kernels (device pointers). */
+int gf_tsc_deposit(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh_dev,
+                   const gf_mesh_desc *mesh_host, float *den);
+int gf_gaussian_smooth(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
+                       const gf_mesh_desc *mesh_dev, float *den);
+int gf_find_den(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh_dev, const float *den,
+                float *densph);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

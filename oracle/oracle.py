@@ -1,0 +1,237 @@
+"""Python bindings of the oracle libraries (test infrastructure only).
+
+* ``Restatement`` — oracle/_build/libgforacle.so, the C restatement
+  (gf_oracle.c) of the reference's TSC / smoothing / findDen / kNN / W4 /
+  tree-potential arithmetic.
+* ``Reference`` — oracle/_ref/libgfref_{fixed,asbuilt}.so, the reference's own
+  NewGalFinder C compiled from its sources by oracle/Makefile, behind the thin
+  harness in oracle/ref/ref_harness.c.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use this.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+RESTATEMENT = HERE / "_build" / "libgforacle.so"
+REF_DIR = HERE / "_ref"
+REF_SOURCE = Path("/root/reference")
+
+_VP, _I, _I64, _F, _D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def build(ref: bool = True) -> None:
+    """Builds the restatement and, when the reference tree is present, the
+    reference libraries (make -C oracle [ref])."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if ref and REF_SOURCE.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+
+
+class Restatement:
+    _lib = None
+
+    def __init__(self):
+        if Restatement._lib is None:
+            if not RESTATEMENT.exists():
+                build(ref=False)
+            L = ctypes.CDLL(str(RESTATEMENT))
+            L.or_tsc.argtypes = [_I64, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I, _I, _D, _D, _D, _D, _I, _I, _I]
+            L.or_find_den.argtypes = [_I64, _VP, _VP, _VP, _VP, _D, _D, _D, _D, _VP, _I, _I, _I]
+            L.or_smooth.argtypes = [_VP, _I, _I, _I, _D, _F, _VP]
+            L.or_knn_brute.argtypes = [_I64, _VP, _VP, _VP, _I, _VP, _VP]
+            L.or_knn_grid.argtypes = [_I64, _VP, _VP, _VP, _I, _VP, _VP]
+            L.or_sph_density.argtypes = [_I64, _I, _VP, _VP]
+            Restatement._lib = L
+        self.L = Restatement._lib
+
+    @staticmethod
+    def mesh_size(nx, ny, nz):
+        return 2 * (nx // 2 + 1) * ny * nz
+
+    def tsc(self, x, y, z, mass, type_, nx, ny, nz, xmin, ymin, zmin, cellsize, ptype=5,
+            acc_double=False, ref_threads=1):
+        den = np.zeros(self.mesh_size(nx, ny, nz), np.float32)
+        x, y, z, mass = (np.ascontiguousarray(a, np.float64) for a in (x, y, z, mass))
+        t = None if type_ is None else np.ascontiguousarray(type_, np.int32)
+        bad = self.L.or_tsc(len(x), _p(x), _p(y), _p(z), _p(mass), _p(t), _p(den), nx, ny, nz,
+                            xmin, ymin, zmin, cellsize, ptype, int(acc_double), int(ref_threads))
+        if bad:
+            raise ValueError("a particle's TSC stencil falls outside the mesh")
+        return den
+
+    def find_den(self, x, y, z, den, nx, ny, nz, xmin, ymin, zmin, cellsize):
+        x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+        den = np.ascontiguousarray(den, np.float32)
+        out = np.zeros(len(x), np.float32)
+        bad = self.L.or_find_den(len(x), _p(x), _p(y), _p(z), _p(out), xmin, ymin, zmin, cellsize,
+                                 _p(den), nx, ny, nz)
+        if bad:
+            raise ValueError("a particle's TSC stencil falls outside the mesh")
+        return out
+
+    def smooth(self, den, nx, ny, nz, cellsize, rg):
+        d = np.array(den, np.float32, copy=True)
+        out64 = np.zeros(len(d), np.float64)
+        self.L.or_smooth(_p(d), nx, ny, nz, cellsize, rg, _p(out64))
+        return d, out64
+
+    def knn(self, x, y, z, k, method="grid"):
+        x, y, z = (np.ascontiguousarray(a, np.float32) for a in (x, y, z))
+        n = len(x)
+        idx = np.zeros((n, k), np.int64)
+        d2 = np.zeros((n, k), np.float64)
+        fn = self.L.or_knn_grid if method == "grid" else self.L.or_knn_brute
+        if fn(n, _p(x), _p(y), _p(z), k, _p(idx), _p(d2)):
+            raise ValueError("k larger than the number of particles")
+        return idx, d2
+
+    def sph_density(self, d2):
+        d2 = np.ascontiguousarray(d2, np.float64)
+        n, k = d2.shape
+        out = np.zeros(n, np.float32)
+        self.L.or_sph_density(n, k, _p(d2), _p(out))
+        return out
+
+
+class Reference:
+    """The reference's own code (compiled from its sources)."""
+    _libs: dict = {}
+
+    def __init__(self, variant: str = "fixed", arena_mb: int = 4096):
+        path = REF_DIR / f"libgfref_{variant}.so"
+        if variant not in Reference._libs:
+            if not path.exists():
+                if REF_SOURCE.exists():
+                    build(ref=True)
+                else:
+                    raise FileNotFoundError(f"{path} was not built (reference tree absent)")
+            L = ctypes.CDLL(str(path))
+            L.ref_init.argtypes = [ctypes.c_longlong]
+            L.ref_set_cosmology.argtypes = [_F, _F, _F, _F, _F]
+            for name in ("ref_get_potentfact", "ref_get_r1kineticfact", "ref_get_r2kineticfact"):
+                getattr(L, name).restype = _D
+            L.ref_GetBGpotent.argtypes = [_D]
+            L.ref_GetBGpotent.restype = _D
+            L.ref_findsphdensity.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP]
+            L.ref_lagFindStellarCore.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP, _VP, _I, _I,
+                                                 _VP, _VP, _VP]
+            L.ref_assign_density_TSC.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I, _I, _D,
+                                                 _D, _D, _D, _I]
+            L.ref_findDen.argtypes = [_I, _VP, _VP, _VP, _VP, _D, _D, _D, _D, _VP, _I, _I, _I]
+            L.ref_gaussian_Smoothing.argtypes = [_VP, _I, _I, _I, _D, _F]
+            L.ref_find_near_all.argtypes = [_I, _VP, _VP, _VP, _VP, _I, _VP, _VP, _VP]
+            L.ref_Self_Halo_Potent.argtypes = [_I, _VP, _VP, _VP, _VP, _VP]
+            L.ref_External_Halo_Potent.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP, _VP, _VP,
+                                                   _VP]
+            L.ref_tree_potential.argtypes = [_I, _VP, _VP, _VP, _VP, _F, _VP]
+            if L.ref_init(arena_mb) != 0:
+                raise RuntimeError("reference arena allocation failed")
+            Reference._libs[variant] = L
+        self.L = Reference._libs[variant]
+
+    @staticmethod
+    def _d(a):
+        return np.ascontiguousarray(a, np.float64)
+
+    def physics(self):
+        return (self.L.ref_get_potentfact(), self.L.ref_get_r1kineticfact(),
+                self.L.ref_get_r2kineticfact())
+
+    def bg_potent(self, mvir):
+        return self.L.ref_GetBGpotent(mvir)
+
+    def findsphdensity(self, x, y, z, mass, k):
+        x, y, z, mass = map(self._d, (x, y, z, mass))
+        n = len(x)
+        idx = np.zeros(n * k, np.int64)
+        dens = np.zeros(n, np.float32)
+        self.L.ref_findsphdensity(n, _p(x), _p(y), _p(z), _p(mass), _p(idx), k, _p(dens))
+        return idx.reshape(n, k), dens
+
+    def find_near_all(self, x, y, z, mass, k):
+        x, y, z = map(self._d, (x, y, z))
+        m = None if mass is None else self._d(mass)
+        n = len(x)
+        idx = np.zeros(n * k, np.int64)
+        d2 = np.zeros(n * k, np.float64)
+        maxr = np.zeros(n, np.float32)
+        self.L.ref_find_near_all(n, _p(x), _p(y), _p(z), _p(m), k, _p(idx), _p(d2), _p(maxr))
+        return idx.reshape(n, k), d2.reshape(n, k), maxr
+
+    def assign_density_TSC(self, x, y, z, mass, type_, nx, ny, nz, xmin, ymin, zmin, cellsize,
+                           ptype=5):
+        x, y, z, mass = map(self._d, (x, y, z, mass))
+        t = np.ascontiguousarray(type_, np.int32)
+        den = np.zeros(2 * (nx // 2 + 1) * ny * nz, np.float32)
+        self.L.ref_assign_density_TSC(len(x), _p(t), _p(x), _p(y), _p(z), _p(mass), _p(den), nx,
+                                      ny, nz, xmin, ymin, zmin, cellsize, ptype)
+        return den
+
+    def findDen(self, x, y, z, den, nx, ny, nz, xmin, ymin, zmin, cellsize):
+        x, y, z = map(self._d, (x, y, z))
+        den = np.ascontiguousarray(den, np.float32)
+        out = np.zeros(len(x), np.float32)
+        self.L.ref_findDen(len(x), _p(x), _p(y), _p(z), _p(out), xmin, ymin, zmin, cellsize,
+                           _p(den), nx, ny, nz)
+        return out
+
+    def gaussian_Smoothing(self, den, nx, ny, nz, cellsize, rg):
+        d = np.array(den, np.float32, copy=True)
+        self.L.ref_gaussian_Smoothing(_p(d), nx, ny, nz, cellsize, rg)
+        return d
+
+    def lagFindStellarCore(self, x, y, z, mass, type_, k, ptype, maxcore=100000):
+        x, y, z, mass = map(self._d, (x, y, z, mass))
+        t = np.ascontiguousarray(type_, np.int32)
+        n = len(x)
+        dens = np.zeros(n, np.float32)
+        idx = np.zeros(n * k, np.int64)
+        ncore = np.zeros(1, np.int32)
+        peak = np.zeros(maxcore, np.int32)
+        xyzd = np.zeros(4 * maxcore, np.float32)
+        self.L.ref_lagFindStellarCore(n, _p(t), _p(x), _p(y), _p(z), _p(mass), k, _p(dens), _p(idx),
+                                      ptype, maxcore, _p(ncore), _p(peak), _p(xyzd))
+        nc = int(ncore[0])
+        return dens, idx.reshape(n, k), peak[:nc], xyzd[:4 * nc].reshape(nc, 4)
+
+    def tree_potential(self, x, y, z, mass_f32, theta2=0.5):
+        x, y, z = map(self._d, (x, y, z))
+        m = np.ascontiguousarray(mass_f32, np.float32)
+        phi = np.zeros(len(x), np.float32)
+        self.L.ref_tree_potential(len(x), _p(x), _p(y), _p(z), _p(m), theta2, _p(phi))
+        return phi
+
+    def Self_Halo_Potent(self, x, y, z, mass_f32):
+        x, y, z = map(self._d, (x, y, z))
+        m = np.ascontiguousarray(mass_f32, np.float32)
+        pe = np.zeros(len(x), np.float32)
+        self.L.ref_Self_Halo_Potent(len(x), _p(x), _p(y), _p(z), _p(m), _p(pe))
+        return pe
+
+    def External_Halo_Potent(self, tx, ty, tz, tmass, sx, sy, sz, smass):
+        tx, ty, tz, sx, sy, sz = map(self._d, (tx, ty, tz, sx, sy, sz))
+        tm = np.ascontiguousarray(tmass, np.float32)
+        sm = np.ascontiguousarray(smass, np.float32)
+        pe = np.zeros(len(tx), np.float32)
+        self.L.ref_External_Halo_Potent(len(tx), _p(tx), _p(ty), _p(tz), _p(tm), _p(pe), len(sx),
+                                        _p(sx), _p(sy), _p(sz), _p(sm))
+        return pe
+
+
+def ref_available() -> bool:
+    return (REF_DIR / "libgfref_fixed.so").exists() or REF_SOURCE.exists()
+
+
+def cpu_threads() -> int:
+    return len(os.sched_getaffinity(0))

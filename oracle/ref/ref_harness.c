@@ -1,0 +1,244 @@
+/* Harness around the reference's own hot-path functions (compiled unmodified
+ * from NewGalFinder/*.c by oracle/ref/Makefile).  It defines the globals the
+ * reference expects from gfind.c (cosmology, potentfact, rank ids), sets up
+ * the reference's stack arena (Memory2.c:Make_Total_Memory) and the potential
+ * spline table (force_spline.mod3.c:81), and exposes plain-array entry points
+ * that ctypes can call.
+ *
+ * Test infrastructure only: used to generate golden fixtures, to pin the
+ * oracle restatement, and as the CPU baseline ("reference" kind).  Never
+ * linked into the product library. */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "Memory.h"
+#include "ramses.h"
+#include "tree.h"
+#include "defs.h"
+#include "params.h"
+
+/* ---- globals normally defined by gfind.c (names renamed by defs.h) ---- */
+int myid = 0, nid = 1;
+double onesolarmass = 1.0;
+double com2real, real2com, potentfact, pntmass, r1kineticfact, r2kineticfact;
+float amax = 1.f, a = 1.f, rng = 1.f, size = 100.f, hubble = 70.f;
+int ng = 0, nspace = 1, nx = 0, ny = 0, nz = 0;
+float omep = 0.3f, omeplam = 0.7f, acoeff[8];
+float epsilon = 0.f;
+float m_tidal[10000], r_tidal[10000]; /* NUM_MASS, header.h:97 */
+
+/* ---- reference functions (signatures from the cited files) ---- */
+typedef struct Vector3d { double x, y, z; } Vector3d; /* subhaloden.mod6.c:70 */
+void i_potent_spline(void);                                          /* force_spline.mod3.c:81 */
+void findsphdensity(SimpleBasicParticleType *, int, long long *, int, float *); /* nnost.c:560 */
+void lagFindStellarCore(SimpleBasicParticleType *, int, int, float *, Coretype **, int *, int,
+                        long long *, int);                           /* nnost.c:991 */
+void assign_density_TSC(SimpleBasicParticleType *, int, float *, int, int, int, double, double,
+                        double, double, int);                        /* tsc_omp2.c:166 */
+void findDen(SimpleBasicParticleType *, int, float *, double, double, double, double, float *,
+             int, int, int);                                         /* tsc_omp2.c:40 */
+void gaussian_Smoothing(float *, int, int, int, double, float);      /* gsmooth.c:14 */
+void new_Make_Tree_Near(TStruct *, size_t, TPtlStruct *, size_t, int); /* nnost.c:199 */
+int Find_Near(particle *, int, TStruct *, TPtlStruct *, float *, long long *, dptype *, float *);
+void Self_Halo_Potent(int, Vector3d *, float *, float *);            /* subhaloden.mod6.c:1477 */
+void External_Halo_Potent(int, Vector3d *, float *, float *, int, Vector3d *, float *);
+double GetBGpotent(double);                                          /* subhaloden.mod6.c:1093 */
+
+static int g_ready = 0;
+
+/* gfind.c:842-890 (physical_parameters), second assignment block, which is
+ * the one that takes effect. */
+static void set_physics(void) {
+    float omepk = 1.f - omep - omeplam;
+    float h0 = hubble / 100.f;
+    float Hsub = sqrt(omep * pow(amax / a, 3) + omeplam + omepk * pow(amax / a, 2));
+    com2real = 1.L / h0 * a / amax * Mpc;
+    real2com = 1.L / com2real;
+    pntmass = Msun / h0;
+    potentfact = 6.672E-8L * pntmass / com2real; /* G from header.h:1 */
+    r1kineticfact = 100.E5L * Hsub * a / amax;
+    r2kineticfact = 1.E5L;
+}
+
+int ref_init(long long megabytes) {
+    if (g_ready) return 0;
+    if (!Make_Total_Memory(megabytes * MEGABYTE)) return -1;
+    i_potent_spline();
+    set_physics();
+    g_ready = 1;
+    return 0;
+}
+
+void ref_set_cosmology(float amax_, float a_, float omep_, float omeplam_, float hubble_) {
+    amax = amax_; a = a_; omep = omep_; omeplam = omeplam_; hubble = hubble_;
+    set_physics();
+}
+
+double ref_get_potentfact(void) { return potentfact; }
+double ref_get_r1kineticfact(void) { return r1kineticfact; }
+double ref_get_r2kineticfact(void) { return r2kineticfact; }
+double ref_GetBGpotent(double mvir) { return GetBGpotent(mvir); }
+
+static SimpleBasicParticleType *make_bp(int np, const int *type, const double *x, const double *y,
+                                        const double *z, const double *mass) {
+    SimpleBasicParticleType *bp = NULL;
+    bp = (SimpleBasicParticleType *)Malloc(sizeof(SimpleBasicParticleType) * (size_t)np, PPTR(bp));
+    for (int i = 0; i < np; i++) {
+        memset(&bp[i], 0, sizeof(bp[i]));
+        bp[i].type = type ? (unsigned)type[i] : TYPE_DM;
+        bp[i].mass = mass ? mass[i] : 1.0;
+        bp[i].x = x[i];
+        bp[i].y = y[i];
+        bp[i].z = z[i];
+        bp[i].indx = i;
+    }
+    return bp;
+}
+
+int ref_findsphdensity(int np, const double *x, const double *y, const double *z,
+                       const double *mass, long long *nearindex, int k, float *dens) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, NULL, x, y, z, mass);
+    findsphdensity(bp, np, nearindex, k, dens);
+    Free(bp);
+    return 0;
+}
+
+/* Runs lagFindStellarCore and returns the per-particle mesh density, the
+ * neighbour lists and the mesh-peak cores (peak index, x, y, z, density). */
+int ref_lagFindStellarCore(int np, const int *type, const double *x, const double *y,
+                           const double *z, const double *mass, int k, float *dens,
+                           long long *nearindex, int ptype, int maxcore, int *ncore,
+                           int *core_peak, float *core_xyzd) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, type, x, y, z, mass);
+    Coretype *core = NULL;
+    core = (Coretype *)Malloc(sizeof(Coretype) * (size_t)maxcore, PPTR(core));
+    int numcore = 0;
+    lagFindStellarCore(bp, np, k, dens, &core, &numcore, maxcore, nearindex, ptype);
+    *ncore = numcore;
+    for (int c = 0; c < numcore; c++) {
+        core_peak[c] = core[c].peak;
+        core_xyzd[4 * c + 0] = core[c].cx;
+        core_xyzd[4 * c + 1] = core[c].cy;
+        core_xyzd[4 * c + 2] = core[c].cz;
+        core_xyzd[4 * c + 3] = core[c].density;
+    }
+    if (numcore > 0) Free(core);
+    Free(bp);
+    return 0;
+}
+
+int ref_assign_density_TSC(int np, const int *type, const double *x, const double *y,
+                           const double *z, const double *mass, float *den, int nx_, int ny_,
+                           int nz_, double xmin, double ymin, double zmin, double cellsize,
+                           int ptype) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, type, x, y, z, mass);
+    assign_density_TSC(bp, np, den, nx_, ny_, nz_, xmin, ymin, zmin, cellsize, ptype);
+    Free(bp);
+    return 0;
+}
+
+int ref_findDen(int np, const double *x, const double *y, const double *z, float *densph,
+                double xmin, double ymin, double zmin, double cellsize, float *den, int nx_,
+                int ny_, int nz_) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, NULL, x, y, z, NULL);
+    findDen(bp, np, densph, xmin, ymin, zmin, cellsize, den, nx_, ny_, nz_);
+    Free(bp);
+    return 0;
+}
+
+int ref_gaussian_Smoothing(float *den, int nx_, int ny_, int nz_, double cellsize, float rg) {
+    if (!g_ready) return -1;
+    gaussian_Smoothing(den, nx_, ny_, nz_, cellsize, rg);
+    return 0;
+}
+
+/* new_Make_Tree_Near + Find_Near for every particle (the findsphdensity
+ * inner loop without the density), returning the raw lists. */
+int ref_find_near_all(int np, const double *x, const double *y, const double *z,
+                      const double *mass, int k, long long *idx, double *d2, float *maxr) {
+    if (!g_ready) return -1;
+    particle *p = NULL;
+    TPtlStruct *ptl = NULL;
+    TStruct *tree = NULL;
+    p = (particle *)Malloc(sizeof(particle) * (size_t)np, PPTR(p));
+    ptl = (TPtlStruct *)Malloc(sizeof(TPtlStruct) * (size_t)np, PPTR(ptl));
+    size_t nnode = (size_t)(np / 2 > 650000 ? np / 2 : 650000);
+    tree = (TStruct *)Malloc(sizeof(TStruct) * nnode, PPTR(tree));
+    for (int i = 0; i < np; i++) {
+        p[i].x = x[i]; p[i].y = y[i]; p[i].z = z[i];
+        ptl[i].type = TYPE_PTL;
+        ptl[i].x = x[i]; ptl[i].y = y[i]; ptl[i].z = z[i];
+        ptl[i].mass = mass ? mass[i] : 1.0;
+    }
+    new_Make_Tree_Near(tree, nnode, ptl, (size_t)np, RECURSIVE);
+#pragma omp parallel for schedule(guided)
+    for (int i = 0; i < np; i++) {
+        float mass_k[MAX_NUM_NEAR];
+        Find_Near(p + i, k, tree, ptl, maxr + i, idx + (size_t)i * k, d2 + (size_t)i * k, mass_k);
+    }
+    Free(tree);
+    Free(ptl);
+    Free(p);
+    return 0;
+}
+
+int ref_Self_Halo_Potent(int np, const double *x, const double *y, const double *z,
+                         float *mass, float *penergy) {
+    if (!g_ready) return -1;
+    Vector3d *r = NULL;
+    r = (Vector3d *)Malloc(sizeof(Vector3d) * (size_t)np, PPTR(r));
+    for (int i = 0; i < np; i++) { r[i].x = x[i]; r[i].y = y[i]; r[i].z = z[i]; }
+    Self_Halo_Potent(np, r, mass, penergy);
+    Free(r);
+    return 0;
+}
+
+int ref_External_Halo_Potent(int nend, const double *x, const double *y, const double *z,
+                             float *mass, float *penergy, int snp, const double *sx,
+                             const double *sy, const double *sz, float *smass) {
+    if (!g_ready) return -1;
+    Vector3d *r = NULL, *sr = NULL;
+    r = (Vector3d *)Malloc(sizeof(Vector3d) * (size_t)nend, PPTR(r));
+    sr = (Vector3d *)Malloc(sizeof(Vector3d) * (size_t)snp, PPTR(sr));
+    for (int i = 0; i < nend; i++) { r[i].x = x[i]; r[i].y = y[i]; r[i].z = z[i]; }
+    for (int i = 0; i < snp; i++) { sr[i].x = sx[i]; sr[i].y = sy[i]; sr[i].z = sz[i]; }
+    External_Halo_Potent(nend, r, mass, penergy, snp, sr, smass);
+    Free(sr);
+    Free(r);
+    return 0;
+}
+
+/* Make_Tree (SERIALIZED, as Self_Halo_Potent builds it) + treeplumpotential at
+ * every particle: the raw tree potential before potentfact and the NFW term. */
+void Make_Tree(TStruct *, size_t, TPtlStruct *, size_t, float, int);
+float treeplumpotential(particle *, float, TStruct *, TPtlStruct *);
+int ref_tree_potential(int np, const double *x, const double *y, const double *z,
+                       const float *mass, float theta2, float *phi) {
+    if (!g_ready) return -1;
+    TPtlStruct *ptl = NULL;
+    TStruct *tree = NULL;
+    size_t nnode = (size_t)(np / 2 > 650000 ? np / 2 : 650000);
+    tree = (TStruct *)Malloc(sizeof(TStruct) * nnode, PPTR(tree));
+    ptl = (TPtlStruct *)Malloc(sizeof(TPtlStruct) * (size_t)np, PPTR(ptl));
+    for (int i = 0; i < np; i++) {
+        ptl[i].type = TYPE_PTL;
+        ptl[i].x = x[i]; ptl[i].y = y[i]; ptl[i].z = z[i];
+        ptl[i].mass = mass[i];
+    }
+    Make_Tree(tree, nnode, ptl, (size_t)np, theta2, SERIALIZED);
+#pragma omp parallel for schedule(guided)
+    for (int i = 0; i < np; i++) {
+        particle p;
+        p.x = x[i]; p.y = y[i]; p.z = z[i];
+        phi[i] = treeplumpotential(&p, theta2, tree, ptl);
+    }
+    Free(ptl);
+    Free(tree);
+    return 0;
+}

@@ -1,0 +1,119 @@
+"""Generates the golden fixtures in tests/golden/ by running the reference's
+own NewGalFinder C code (compiled from /root/reference by oracle/Makefile,
+with the one-token INSERT fix for the "fixed" variant and the FP64 fftw3f
+shim standing in for FFTW) on small seeded inputs.
+
+    python tests/golden/make_golden.py
+
+The reference runs single-threaded (OMP_NUM_THREADS=1) so that its float
+accumulations happen in particle order and the fixtures are reproducible.
+Fixtures hold the inputs as well as the outputs, so tests never need the
+reference tree.  Test infrastructure only.
+"""
+from __future__ import annotations
+
+import os
+import sys
+from pathlib import Path
+
+os.environ["OMP_NUM_THREADS"] = "1"
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+from oracle.oracle import Reference  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+CELL, NBUFF, RG = 0.004, 10, 0.008
+
+
+def blob(seed, n, sigma, nsub=2):
+    """Clustered test halo: a Gaussian core plus two compact clumps, positions
+    recentred as Dump2BP does (x - min)."""
+    rng = np.random.default_rng(seed)
+    parts = [sigma * rng.standard_normal((n - 2 * (n // 8), 3))]
+    for _ in range(nsub):
+        c = sigma * 1.5 * rng.standard_normal(3)
+        parts.append(c + 0.2 * sigma * rng.standard_normal((n // 8, 3)))
+    p = np.concatenate(parts)[:n]
+    p -= p.min(axis=0)
+    return p
+
+
+def ref_mesh(p):
+    """lagFindStellarCore's mesh for recentred positions (nnost.c:1040-1059)."""
+    xmax = p.max(axis=0)
+    xmax = xmax + xmax * 0.0001
+    n = (xmax / CELL + NBUFF).astype(int)
+    origin = 0.0 - CELL * NBUFF / 2.0
+    return int(n[0]), int(n[1]), int(n[2]), origin
+
+
+def main():
+    ref = Reference("fixed")
+    ref_asbuilt = Reference("asbuilt")
+
+    # ---- mesh chain: TSC (all / stars) -> smoothing -> findDen
+    p = blob(11, 2000, 0.012)
+    rng = np.random.default_rng(12)
+    mass = 10 ** rng.uniform(6, 8, len(p))
+    typ = np.where(rng.random(len(p)) < 0.3, 1, 2).astype(np.int32)
+    nx, ny, nz, o = ref_mesh(p)
+    out = dict(pos=p, mass=mass, type=typ, dims=np.array([nx, ny, nz]), origin=o, cell=CELL, rg=RG)
+    for tag, ptype in (("all", 5), ("star", 1)):
+        den = ref.assign_density_TSC(p[:, 0], p[:, 1], p[:, 2], mass, typ, nx, ny, nz, o, o, o,
+                                     CELL, ptype)
+        sm = ref.gaussian_Smoothing(den, nx, ny, nz, CELL, RG)
+        dens = ref.findDen(p[:, 0], p[:, 1], p[:, 2], sm, nx, ny, nz, o, o, o, CELL)
+        out[f"tsc_{tag}"] = den
+        out[f"smooth_{tag}"] = sm
+        out[f"findden_{tag}"] = dens
+    ldens, lidx, lpeak, lcore = ref.lagFindStellarCore(p[:, 0], p[:, 1], p[:, 2], mass, typ, 32, 5)
+    out["lag_dens_all"] = ldens
+    np.savez_compressed(OUT / "mesh_chain.npz", **out)
+
+    # ---- smoothing on odd / prime mesh sizes with random content
+    rng = np.random.default_rng(13)
+    sm_out = {}
+    for (a, b, c) in ((23, 29, 31), (16, 12, 20)):
+        mx = 2 * (a // 2 + 1)
+        den = np.zeros((c, b, mx), np.float32)
+        den[:, :, :a] = rng.random((c, b, a)).astype(np.float32) ** 8 * 1e4
+        den = den.ravel()
+        sm_out[f"in_{a}_{b}_{c}"] = den
+        sm_out[f"out_{a}_{b}_{c}"] = ref.gaussian_Smoothing(den, a, b, c, CELL, 0.006)
+    np.savez_compressed(OUT / "smooth_sizes.npz", **sm_out)
+
+    # ---- kNN + SPH density (findsphdensity): fixed and as-built
+    q = blob(21, 2000, 0.05).astype(np.float32).astype(np.float64)  # FP32-rounded positions
+    m = np.full(len(q), 1e8)
+    idx_f, dens_f = ref.findsphdensity(q[:, 0], q[:, 1], q[:, 2], m, 32)
+    idx_a, dens_a = ref_asbuilt.findsphdensity(q[:, 0], q[:, 1], q[:, 2], m, 32)
+    fidx, fd2, fmaxr = ref.find_near_all(q[:, 0], q[:, 1], q[:, 2], m, 32)
+    np.savez_compressed(OUT / "knn.npz", pos=q, idx_fixed=idx_f.astype(np.int32), dens_fixed=dens_f,
+                        idx_asbuilt=idx_a.astype(np.int32), dens_asbuilt=dens_a,
+                        maxr_fixed=fmaxr)
+
+    # ---- tree potential, Self_Halo_Potent, External_Halo_Potent
+    r = blob(31, 3000, 0.05)
+    rng = np.random.default_rng(32)
+    mf = (10 ** rng.uniform(7, 8.5, len(r))).astype(np.float32)
+    phi = ref.tree_potential(r[:, 0], r[:, 1], r[:, 2], mf, 0.5)
+    self_pe = ref.Self_Halo_Potent(r[:, 0], r[:, 1], r[:, 2], mf)
+    small = r[:80]
+    self_small = ref.Self_Halo_Potent(small[:, 0], small[:, 1], small[:, 2], mf[:80])
+    tgt = r[::3][:1500]
+    ext_pe = ref.External_Halo_Potent(tgt[:, 0], tgt[:, 1], tgt[:, 2], mf[::3][:1500], r[:, 0],
+                                      r[:, 1], r[:, 2], mf)
+    potentfact, r1k, r2k = ref.physics()
+    np.savez_compressed(OUT / "potential.npz", pos=r, mass=mf, phi_tree=phi, self_pe=self_pe,
+                        self_small=self_small, ext_pe=ext_pe, potentfact=potentfact,
+                        r1kineticfact=r1k, r2kineticfact=r2k,
+                        bg_1e12=ref.bg_potent(1e12), bg_mass=ref.bg_potent(float(np.sum(mf, dtype=np.float64))))
+    for f in sorted(OUT.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()
