@@ -1,0 +1,115 @@
+"""Python mirror of the reference entry points that libgf replaces.
+
+Each function takes the reference's arguments (numpy arrays in place of the C
+pointers, with the reference's struct layouts from ``_lib``) and calls the
+drop-in symbol of the same name in libgf.so.  Where the reference prints a
+message and calls exit(), these raise ``GFError``.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from ._lib import BP_DTYPE, VEC3_DTYPE, check_last, lib, ptr
+
+
+def mesh_floats(nx: int, ny: int, nz: int) -> int:
+    """Length of a padded r2c mesh, mx*ny*nz with mx = 2(nx/2+1) (tsc_omp2.c:16,198)."""
+    return 2 * (nx // 2 + 1) * ny * nz
+
+
+def _bp(bp: np.ndarray) -> np.ndarray:
+    if bp.dtype != BP_DTYPE or not bp.flags.c_contiguous:
+        raise TypeError("bp must be a contiguous SimpleBasicParticleType array (BP_DTYPE)")
+    return bp
+
+
+def assign_density_TSC(bp, nx, ny, nz, Xmin, Ymin, Zmin, cellsize, ptype, den=None):
+    """tsc_omp2.c:166 — TSC deposit of bp into a zeroed mesh (returned)."""
+    bp = _bp(bp)
+    if den is None:
+        den = np.zeros(mesh_floats(nx, ny, nz), np.float32)
+    lib().assign_density_TSC(ptr(bp), len(bp), ptr(den), nx, ny, nz, Xmin, Ymin, Zmin, cellsize,
+                             ptype)
+    check_last()
+    return den
+
+
+def findDen(bp, den, nx, ny, nz, xmin, ymin, zmin, cellsize):
+    """tsc_omp2.c:40 — TSC-weighted mesh value at every particle."""
+    bp = _bp(bp)
+    den = np.ascontiguousarray(den, np.float32)
+    out = np.zeros(len(bp), np.float32)
+    lib().findDen(ptr(bp), len(bp), ptr(out), xmin, ymin, zmin, cellsize, ptr(den), nx, ny, nz)
+    check_last()
+    return out
+
+
+def gaussian_Smoothing(den, nx, ny, nz, cellsize, RG):
+    """gsmooth.c:14 — in-place Gaussian smoothing of a padded mesh."""
+    if den.dtype != np.float32 or not den.flags.c_contiguous:
+        raise TypeError("den must be a contiguous float32 array")
+    lib().gaussian_Smoothing(ptr(den), nx, ny, nz, cellsize, RG)
+    check_last()
+    return den
+
+
+def findsphdensity(bp, numnear):
+    """nnost.c:560 — k nearest neighbours (self included) and the W4 density."""
+    bp = _bp(bp)
+    n = len(bp)
+    near = np.zeros((n, numnear), np.int64)
+    dens = np.zeros(n, np.float32)
+    lib().findsphdensity(ptr(bp), n, ptr(near), numnear, ptr(dens))
+    check_last()
+    return near, dens
+
+
+def _vec3(r) -> np.ndarray:
+    r = np.asarray(r)
+    if r.dtype == VEC3_DTYPE:
+        return np.ascontiguousarray(r)
+    r = np.ascontiguousarray(r, np.float64).reshape(-1, 3)
+    return r.view(VEC3_DTYPE).reshape(-1)
+
+
+def Self_Halo_Potent(r, mass):
+    """subhaloden.mod6.c:1477 — self-potential energy of a member set."""
+    r = _vec3(r)
+    mass = np.ascontiguousarray(mass, np.float32)
+    pe = np.zeros(len(r), np.float32)
+    lib().Self_Halo_Potent(len(r), ptr(r), ptr(mass), ptr(pe))
+    check_last()
+    return pe
+
+
+def External_Halo_Potent(r, mass, sr, smass):
+    """subhaloden.mod6.c:1537 — potential of the sources (sr, smass) at r."""
+    r, sr = _vec3(r), _vec3(sr)
+    mass = np.ascontiguousarray(mass, np.float32)
+    smass = np.ascontiguousarray(smass, np.float32)
+    pe = np.zeros(len(r), np.float32)
+    lib().External_Halo_Potent(len(r), ptr(r), ptr(mass), ptr(pe), len(sr), ptr(sr), ptr(smass))
+    check_last()
+    return pe
+
+
+def i_potent_spline():
+    """force_spline.mod3.c:81 — no table is needed by the GPU kernel."""
+    lib().i_potent_spline()
+    check_last()
+
+
+def physics() -> dict:
+    ph = _lib.Physics()
+    _lib.check(lib().gf_get_physics(ph))
+    return {f: getattr(ph, f) for f, _ in _lib.Physics._fields_}
+
+
+def set_cosmology(amax=1.0, a=1.0, omep=0.3, omeplam=0.7, hubble=70.0):
+    _lib.check(lib().gf_set_cosmology(amax, a, omep, omeplam, hubble))
+
+
+def bg_potent(mvir: float) -> float:
+    """GetBGpotent, subhaloden.mod6.c:1093."""
+    return lib().gf_bg_potent(mvir)
