@@ -67,6 +67,50 @@ class Physics(ctypes.Structure):
     ]
 
 
+class TreeInfo(ctypes.Structure):
+    _fields_ = [("nparticle", ctypes.c_int64), ("nhalo", ctypes.c_int32), ("nnode", ctypes.c_int32)]
+
+
+class StageConfig(ctypes.Structure):
+    _fields_ = [
+        ("mesh", MeshRule), ("box", ctypes.c_double), ("knn_k", ctypes.c_int32),
+        ("do_mesh", ctypes.c_int32), ("do_potential", ctypes.c_int32), ("ndirect", ctypes.c_int32),
+        ("theta2", ctypes.c_float), ("add_bg", ctypes.c_int32), ("q5_asbuilt", ctypes.c_int32),
+        ("reserved", ctypes.c_int32), ("potentfact", ctypes.c_double),
+    ]
+
+
+class StageOut(ctypes.Structure):
+    _fields_ = [
+        ("nearindex", ctypes.c_void_p), ("dens_sph", ctypes.c_void_p),
+        ("dens_mesh", ctypes.c_void_p), ("penergy", ctypes.c_void_p), ("xr", ctypes.c_void_p),
+        ("yr", ctypes.c_void_p), ("zr", ctypes.c_void_p),
+    ]
+
+
+class StageStats(ctypes.Structure):
+    _fields_ = [
+        ("nparticle", ctypes.c_int64), ("nnode", ctypes.c_int64), ("mesh_cells", ctypes.c_int64),
+        ("nhalo", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("pp_interactions", ctypes.c_uint64), ("pc_interactions", ctypes.c_uint64),
+        ("ms_recentre", ctypes.c_float), ("ms_tree", ctypes.c_float), ("ms_knn", ctypes.c_float),
+        ("ms_tsc", ctypes.c_float), ("ms_smooth", ctypes.c_float), ("ms_findden", ctypes.c_float),
+        ("ms_potential", ctypes.c_float), ("ms_pad", ctypes.c_float),
+    ]
+
+
+# preorder node records exported by gf_tree_export
+BH_NODE_DTYPE = np.dtype([
+    ("com", "<f8", (3,)), ("open_r2", "<f8"), ("mass", "<f4"), ("trq", "<f4"), ("q", "<f4", (6,)),
+    ("skip", "<i4"), ("lstart", "<i4"), ("lcount", "<i4"), ("count", "<i4"),
+])
+KNN_NODE_DTYPE = np.dtype([
+    ("lo", "<f4", (3,)), ("hi", "<f4", (3,)), ("skip", "<i4"), ("lstart", "<i4"),
+    ("lcount", "<i4"), ("count", "<i4"),
+])
+assert BH_NODE_DTYPE.itemsize == 80 and KNN_NODE_DTYPE.itemsize == 40
+
+
 class GFError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"libgf status {status}: {msg}")
@@ -103,6 +147,12 @@ SIGNATURES = {
     "gf_tsc_deposit": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP]),
     "gf_gaussian_smooth": (_INT, [_VP, _I32, _VP, _VP, _VP]),
     "gf_find_den": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP]),
+    "gf_tree_build": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _INT, ctypes.POINTER(TreeInfo)]),
+    "gf_tree_export": (_INT, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "gf_knn_density": (_INT, [_VP, _I32, _I64, _VP, _VP, _INT, _VP, _VP]),
+    "gf_self_potential": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _I32, _D, _INT, _VP, _VP]),
+    "gf_stage_run": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),
+                            ctypes.POINTER(StageOut), ctypes.POINTER(StageStats)]),
 }
 
 

@@ -88,3 +88,101 @@ def mesh_stage(ctx: Context, batch: DeviceBatch, mesh: np.ndarray, total: int, s
     check(lib().gf_mesh_stage(ctx.handle, ctypes.byref(b), ptr(mesh_dev), ptr(mesh), ptr(den),
                               ptr(densph), int(smooth)))
     return den, densph
+
+
+def _pos4(x, y, z, m, device):
+    p = np.stack([np.asarray(x, np.float32), np.asarray(y, np.float32),
+                  np.asarray(z, np.float32), np.asarray(m, np.float32)], 1)
+    return torch.as_tensor(np.ascontiguousarray(p), device=device)
+
+
+def tree_build_export(ctx: Context, pstart, pos4, theta2=0.5, q5_asbuilt=False) -> dict:
+    """Builds the octree of FP32 recentred positions (pos4: (n, 4) x, y, z, mass;
+    torch tensor on the device or numpy) and returns it in host memory."""
+    dev = torch.device("cuda", ctx.device)
+    pos4 = torch.as_tensor(pos4, dtype=torch.float32, device=dev).contiguous()
+    ps = torch.as_tensor(np.asarray(pstart, np.int64), device=dev)
+    info = _lib.TreeInfo()
+    n, nh = pos4.shape[0], ps.numel() - 1
+    check(lib().gf_tree_build(ctx.handle, nh, n, ptr(ps), ptr(pos4), theta2, int(q5_asbuilt),
+                              ctypes.byref(info)))
+    nn = info.nnode
+    bh = np.zeros(nn, _lib.BH_NODE_DTYPE)
+    kn = np.zeros(nn, _lib.KNN_NODE_DTYPE)
+    tpos = np.zeros((n, 4), np.float32)
+    perm = np.zeros(n, np.int32)
+    root = np.zeros(nh, np.int32)
+    rend = np.zeros(nh, np.int32)
+    check(lib().gf_tree_export(ctx.handle, ptr(bh), ptr(kn), ptr(tpos), ptr(perm), ptr(root),
+                               ptr(rend)))
+    return dict(bh=bh, knn=kn, pos=tpos, perm=perm, root=root, rend=rend, nnode=nn)
+
+
+def knn_density(ctx: Context, pstart, pos4, k=32):
+    """k nearest neighbours (halo-local indices) and W4 density per particle."""
+    dev = torch.device("cuda", ctx.device)
+    pos4 = torch.as_tensor(pos4, dtype=torch.float32, device=dev).contiguous()
+    ps = torch.as_tensor(np.asarray(pstart, np.int64), device=dev)
+    n = pos4.shape[0]
+    near = torch.empty((n, k), dtype=torch.int32, device=dev)
+    dens = torch.empty(n, dtype=torch.float32, device=dev)
+    check(lib().gf_knn_density(ctx.handle, ps.numel() - 1, n, ptr(ps), ptr(pos4), k, ptr(near),
+                               ptr(dens)))
+    return near, dens
+
+
+def self_potential(ctx: Context, pstart, pos4, theta2=0.5, ndirect=0, potentfact=0.0,
+                   add_bg=False):
+    """Returns (penergy, raw potential) for every particle of every halo."""
+    dev = torch.device("cuda", ctx.device)
+    pos4 = torch.as_tensor(pos4, dtype=torch.float32, device=dev).contiguous()
+    ps = torch.as_tensor(np.asarray(pstart, np.int64), device=dev)
+    n = pos4.shape[0]
+    pe = torch.empty(n, dtype=torch.float32, device=dev)
+    raw = torch.empty(n, dtype=torch.float32, device=dev)
+    check(lib().gf_self_potential(ctx.handle, ps.numel() - 1, n, ptr(ps), ptr(pos4), theta2,
+                                  ndirect, potentfact, int(add_bg), ptr(pe), ptr(raw)))
+    return pe, raw
+
+
+def stage_config(mesh: MeshRule | None = None, box=100.0, knn_k=32, do_mesh=True,
+                 do_potential=True, ndirect=100, theta2=0.5, add_bg=True, q5_asbuilt=False,
+                 potentfact=0.0) -> _lib.StageConfig:
+    if mesh is None:
+        mesh = mesh_rule(mode=_lib.MESH_POW2, rg=2.0, rg_in_cells=True)
+    return _lib.StageConfig(mesh, box, knn_k, int(do_mesh), int(do_potential), ndirect, theta2,
+                            int(add_bg), int(q5_asbuilt), 0, potentfact)
+
+
+class StageBuffers:
+    """Device outputs of gf_stage_run for a batch of n particles."""
+
+    def __init__(self, n: int, k: int, device, keep_positions=False):
+        self.nearindex = torch.empty((n, max(k, 1)), dtype=torch.int32, device=device)
+        self.dens_sph = torch.empty(n, dtype=torch.float32, device=device)
+        self.dens_mesh = torch.empty(n, dtype=torch.float32, device=device)
+        self.penergy = torch.empty(n, dtype=torch.float32, device=device)
+        self.xr = self.yr = self.zr = None
+        if keep_positions:
+            self.xr = torch.empty(n, dtype=torch.float64, device=device)
+            self.yr = torch.empty(n, dtype=torch.float64, device=device)
+            self.zr = torch.empty(n, dtype=torch.float64, device=device)
+
+    def c(self) -> _lib.StageOut:
+        return _lib.StageOut(ptr(self.nearindex), ptr(self.dens_sph), ptr(self.dens_mesh),
+                             ptr(self.penergy), ptr(self.xr), ptr(self.yr), ptr(self.zr))
+
+
+def stage_run(ctx: Context, batch: DeviceBatch, cfg: _lib.StageConfig,
+              out: StageBuffers | None = None, stats=False):
+    """Runs the whole density-and-potential stage on the batch."""
+    if out is None:
+        out = StageBuffers(batch.n, cfg.knn_k, batch.x.device, keep_positions=True)
+    st = _lib.StageStats() if stats else None
+    b = batch.c()
+    oc = out.c()
+    check(lib().gf_stage_run(ctx.handle, ctypes.byref(b), ctypes.byref(cfg), ctypes.byref(oc),
+                             ctypes.byref(st) if st is not None else None))
+    if stats:
+        return out, {f: getattr(st, f) for f, _ in _lib.StageStats._fields_}
+    return out

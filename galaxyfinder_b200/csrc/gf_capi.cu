@@ -517,16 +517,3 @@ void i_potent_spline(void) {
 
 }  // extern "C"
 
-// Entry points whose kernels land in the next translation units.
-extern "C" {
-__attribute__((weak)) void findsphdensity(SimpleBasicParticleType *, int, long long *, int, float *) {
-    set_status(GF_ENOTIMPL, "findsphdensity: not built");
-}
-__attribute__((weak)) void Self_Halo_Potent(int, Vector3d *, float *, float *) {
-    set_status(GF_ENOTIMPL, "Self_Halo_Potent: not built");
-}
-__attribute__((weak)) void External_Halo_Potent(int, Vector3d *, float *, float *, int, Vector3d *,
-                                                float *) {
-    set_status(GF_ENOTIMPL, "External_Halo_Potent: not built");
-}
-}

@@ -75,6 +75,40 @@ struct HostPinned {
     template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+// ---------------------------------------------------------------- octree
+// Node of the kNN walk (preorder).  lo/hi is the exact FP32 bounding box of
+// every particle in the subtree; loose particles are those of the node's
+// octants that were not divided (fewer than 10 particles).
+struct KnnNode {
+    float lo[3], hi[3];
+    int32_t skip;    // preorder index just past this subtree
+    int32_t lstart;  // first loose particle (tree order)
+    int32_t lcount;
+    int32_t count;   // particles in the subtree: [lstart, lstart + count)
+};
+
+// Node of the potential walk (preorder): monopole + quadrupole about the
+// centre of mass, opening radius^2 = dist2/theta2 (ost.c:72-83, 557-582).
+struct BhNode {
+    double com[3];
+    double open_r2;
+    float mass, trq;
+    float q[6];  // xx, yy, zz, xy, xz, yz second moments about the COM
+    int32_t skip, lstart, lcount, count;
+};
+
+struct TreeView {
+    int32_t nhalo = 0, nnode = 0;
+    int64_t n = 0;
+    const float4 *pos = nullptr;   // tree order (x, y, z, mass)
+    const int32_t *perm = nullptr; // tree order -> batch index
+    const int32_t *root = nullptr; // [nhalo] preorder root of halo h
+    const int32_t *rend = nullptr; // [nhalo] preorder end of halo h
+    const KnnNode *knn = nullptr;
+    const BhNode *bh = nullptr;
+    const int32_t *phalo = nullptr; // tree order -> halo
+};
+
 }  // namespace gf
 
 struct gf_ctx {
@@ -86,6 +120,7 @@ struct gf_ctx {
     gf::DevBuf hid, mesh, smooth_tiles, smooth_tables, particles, tmp[8];
     gf::DevBuf tree[16];
     gf::HostPinned pin[4];
+    gf::TreeView last_tree;  // the most recent build_tree() on this context
     std::mutex lock;
 };
 

@@ -1,0 +1,218 @@
+// Barnes-Hut potential on the centre-of-mass octree.
+//
+// Reference: NewGalFinder/ost.c:226-251 (treeplumpotential) with the cell
+// term CELLPLUMPOTENT (:144-176) and the particle term PARTICLEPLUMPOTENT
+// (:178-193), opening test treeopen (:72-83): a node is opened when
+// |p - com|^2 < dist2/theta2.  The cell term is
+//     -M/r + trQ/(2 r^3) - 3 (d.Q.d)/(2 r^5)
+// which the reference reads from linearly interpolated tables of -1/x,
+// 1/(2x^3) and -3/(2x^5) (force_spline.mod3.c:81-138); here it is evaluated
+// directly.  The drivers Self_Halo_Potent / External_Halo_Potent
+// (subhaloden.mod6.c:1477-1621) use a direct sum below 100 members (self) or
+// 1000 targets (external), then scale by potentfact and add the NFW
+// background term of the halo mass (GetBGpotent, :1093-1101).
+//
+// One thread per target.  The 32 targets of a warp are neighbours in tree
+// order and walk the preorder node array in lockstep: every iteration the warp
+// takes the smallest next-node index among its lanes, and the lanes waiting
+// at that node apply their own opening decision (open: sum the node's loose
+// particles and continue at i + 1; accept: add the cell term and continue at
+// skip[i]).  Opening decisions use the same FP64 |p - com|^2 as the
+// reference, so they are identical to an FP64 walk of the same tree; the
+// terms are FP32 evaluated from exact FP64 position differences and summed
+// with Kahan compensation.
+#include <float.h>
+#include <limits.h>
+#include <math.h>
+
+#include <algorithm>
+
+#include "gf_tree.cuh"
+
+namespace gf {
+
+namespace {
+
+struct Kahan {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float v) {
+        const float y = v - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+// GetBGpotent, subhaloden.mod6.c:1059-1101
+__device__ double bg_potent_dev(double mvir, const PotentialParams &pp) {
+    const double G = 6.672E-8, RHOC = 2.7755E11;
+    const double redshift = (double)(pp.amax / pp.a) - 1.0;
+    const double c = 14.5 * pow(mvir / 1.3E13, -0.15) / (1.0 + redshift);
+    const double gc = 1. / (log(1.0 + c) - c / (1.0 + c));
+    const double om = pp.omep;
+    const double vv = 18.0 * M_PI * M_PI + 82.0 * (om - 1.0) - 39.0 * pow(om - 1.0, 2.0);
+    const double rvir = pow(3. * mvir / (4.0 * M_PI * vv * RHOC), 0.3333333333333);
+    const double vc2 = G * mvir / rvir * pp.potentfact;
+    return vc2 * (1 - gc * log(1 + c));
+}
+
+__global__ void __launch_bounds__(128)
+bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__restrict__ thalo,
+          const int32_t *__restrict__ tout, const float4 *__restrict__ spos,
+          const int32_t *__restrict__ root, const int32_t *__restrict__ rend,
+          const BhNode *__restrict__ nodes, const int32_t *__restrict__ direct,
+          const double *__restrict__ bg, PotentialParams pp, float *__restrict__ out,
+          float *__restrict__ raw, unsigned long long *__restrict__ counters) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp0 = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32;
+    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long npp = 0, npc = 0;
+    for (int64_t base = warp0; base < ntarget; base += wstride) {
+        const int64_t t = base + lane;
+        const bool valid = t < ntarget;
+        int h = 0, my = INT_MAX, my_end = 0, always_open = 0;
+        float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (valid) {
+            h = thalo[t];
+            my = root[h];
+            my_end = rend[h];
+            if (my >= my_end) my = INT_MAX;
+            always_open = direct ? direct[h] : 0;
+            P = tpos[t];
+        }
+        const double px = P.x, py = P.y, pz = P.z;
+        Kahan acc;
+        while (true) {
+            const int i = (int)__reduce_min_sync(0xffffffffu, (unsigned)my);
+            if (i == INT_MAX) break;
+            if (my == i) {
+                const BhNode &nd = nodes[i];
+                const double dx = px - nd.com[0];
+                const double dy = py - nd.com[1];
+                const double dz = pz - nd.com[2];
+                // separately rounded, as the reference's treeopen (ost.c:79)
+                const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                            __dmul_rn(dz, dz));
+                if (always_open || d2 < nd.open_r2) {
+                    const int l1 = nd.lstart + nd.lcount;
+                    for (int j = nd.lstart; j < l1; j++) {
+                        const float4 S = spos[j];
+                        // ost.c:186-191: float offsets from FP64 positions
+                        const float fx = (float)(px - (double)S.x);
+                        const float fy = (float)(py - (double)S.y);
+                        const float fz = (float)(pz - (double)S.z);
+                        const float r2 = fx * fx + fy * fy + fz * fz;
+                        if (r2 > 0.f) acc.add(-S.w * rsqrtf(r2));
+                    }
+                    npp += nd.lcount;
+                    my = i + 1;
+                } else {
+                    const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+                    const float r2 = fx * fx + fy * fy + fz * fz;
+                    const float inv = rsqrtf(r2);
+                    const float inv2 = inv * inv;
+                    const float inv3 = inv * inv2;
+                    const float qxy = nd.q[0] * fx * fx + nd.q[1] * fy * fy + nd.q[2] * fz * fz +
+                                      2.f * (nd.q[3] * fx * fy + nd.q[4] * fx * fz + nd.q[5] * fy * fz);
+                    acc.add(-nd.mass * inv + 0.5f * nd.trq * inv3 - 1.5f * qxy * inv3 * inv2);
+                    npc++;
+                    my = nd.skip;
+                }
+                if (my >= my_end) my = INT_MAX;
+            }
+        }
+        if (valid) {
+            const int64_t o = tout ? tout[t] : t;
+            const float phi = acc.s + (-acc.c);
+            if (raw) raw[o] = phi;
+            if (out) {
+                double e = pp.potentfact != 0.0 ? (double)phi * pp.potentfact : (double)phi;
+                if (pp.add_bg && bg) e += bg[h];
+                out[o] = (float)e;  // penergy = potent*potentfact + halobgpotent
+            }
+        }
+    }
+    if (counters) {
+        for (int off = 16; off; off >>= 1) {
+            npp += __shfl_xor_sync(0xffffffffu, npp, off);
+            npc += __shfl_xor_sync(0xffffffffu, npc, off);
+        }
+        if (lane == 0) {
+            atomicAdd(counters + 0, npp);
+            atomicAdd(counters + 1, npc);
+        }
+    }
+}
+
+// Per-halo total mass (FP64 sum of the float masses, as Self_Halo_Potent's
+// Mvir += mass[i]) and background term.
+__global__ void halo_bg_kernel(int32_t nhalo, const int64_t *__restrict__ pstart,
+                               const float4 *__restrict__ pos, PotentialParams pp,
+                               const int32_t *__restrict__ ntarget_halo,
+                               int32_t ndirect, double *__restrict__ bg,
+                               int32_t *__restrict__ direct) {
+    const int h = blockIdx.x;
+    if (h >= nhalo) return;
+    double s = 0.0;
+    for (int64_t p = pstart[h] + threadIdx.x; p < pstart[h + 1]; p += blockDim.x) s += (double)pos[p].w;
+    __shared__ double red[256];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        bg[h] = pp.add_bg ? bg_potent_dev(red[0], pp) : 0.0;
+        const int64_t nt = ntarget_halo ? ntarget_halo[h] : pstart[h + 1] - pstart[h];
+        direct[h] = nt < ndirect ? 1 : 0;
+    }
+}
+
+}  // namespace
+
+// Potential at every particle of every halo from the halo's own tree
+// (self potential); outputs in batch order.
+int launch_self_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart,
+                          const PotentialParams &pp, float *penergy, float *raw,
+                          unsigned long long *counters) {
+    if (t.n <= 0) return GF_OK;
+    GF_TRY(ctx->tmp[5].reserve(((size_t)t.nhalo * (sizeof(double) + sizeof(int32_t))) + 512));
+    double *bg = ctx->tmp[5].as<double>();
+    int32_t *direct = reinterpret_cast<int32_t *>(bg + t.nhalo);
+    // tree-ordered positions carry the masses; halo h is still [pstart[h], pstart[h+1])
+    halo_bg_kernel<<<t.nhalo, 256, 0, ctx->stream>>>(t.nhalo, pstart, t.pos, pp, nullptr,
+                                                     pp.ndirect, bg, direct);
+    GF_LAUNCH_CHECK();
+    const int block = 128;
+    int64_t grid = (t.n + block - 1) / block;
+    grid = std::min<int64_t>(grid, 148LL * 16);
+    bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(t.n, t.pos, t.phalo, t.perm, t.pos, t.root,
+                                                    t.rend, t.bh, direct, bg, pp, penergy, raw,
+                                                    counters);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
+// Potential of one source tree (halo 0 of t) at arbitrary targets.
+int launch_external_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart_src,
+                              int64_t ntarget, const float4 *tpos, const int32_t *thalo,
+                              const int32_t *ntarget_halo, const PotentialParams &pp,
+                              float *penergy, float *raw) {
+    if (ntarget <= 0) return GF_OK;
+    GF_TRY(ctx->tmp[5].reserve(((size_t)t.nhalo * (sizeof(double) + sizeof(int32_t))) + 512));
+    double *bg = ctx->tmp[5].as<double>();
+    int32_t *direct = reinterpret_cast<int32_t *>(bg + t.nhalo);
+    halo_bg_kernel<<<t.nhalo, 256, 0, ctx->stream>>>(t.nhalo, pstart_src, t.pos, pp, ntarget_halo,
+                                                     pp.ndirect, bg, direct);
+    GF_LAUNCH_CHECK();
+    const int block = 128;
+    int64_t grid = std::min<int64_t>((ntarget + block - 1) / block, 148LL * 16);
+    bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, nullptr, t.pos, t.root,
+                                                    t.rend, t.bh, direct, bg, pp, penergy, raw,
+                                                    nullptr);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
+}  // namespace gf

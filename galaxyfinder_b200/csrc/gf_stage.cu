@@ -1,0 +1,400 @@
+// The batched density-and-potential stage and the remaining C-ABI entry
+// points (kNN/SPH density, tree potential, their reference-signature drop-ins).
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gf_tree.cuh"
+
+namespace gf {
+
+namespace {
+
+__global__ void pack_pos_kernel(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
+                                const double *__restrict__ z, const float *__restrict__ mf,
+                                const double *__restrict__ md, float4 *__restrict__ pos) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x)
+        pos[p] = make_float4((float)x[p], (float)y[p], (float)z[p],
+                             mf ? mf[p] : (md ? (float)md[p] : 1.f));
+}
+
+__global__ void vec3_pos_kernel(int64_t n, const double *__restrict__ r, const float *__restrict__ m,
+                                float4 *__restrict__ pos) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+         p += (int64_t)gridDim.x * blockDim.x)
+        pos[p] = make_float4((float)r[3 * p], (float)r[3 * p + 1], (float)r[3 * p + 2], m ? m[p] : 0.f);
+}
+
+int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+PotentialParams potential_params(float theta2, int ndirect, double potentfact, int add_bg) {
+    const gf_physics &ph = physics();
+    PotentialParams pp;
+    pp.theta2 = theta2;
+    pp.ndirect = ndirect;
+    pp.potentfact = potentfact;
+    pp.add_bg = add_bg;
+    pp.amax = ph.amax;
+    pp.a = ph.a;
+    pp.omep = ph.omep;
+    return pp;
+}
+
+struct EventTimer {
+    cudaStream_t s;
+    bool on;
+    cudaEvent_t ev[16];
+    int n = 0;
+    EventTimer(cudaStream_t s_, bool on_) : s(s_), on(on_) {
+        if (on)
+            for (auto &e : ev) cudaEventCreate(&e);
+    }
+    ~EventTimer() {
+        if (on)
+            for (auto &e : ev) cudaEventDestroy(e);
+    }
+    void mark() {
+        if (on && n < 16) cudaEventRecord(ev[n++], s);
+    }
+    float ms(int i) {
+        float t = 0;
+        if (on && i + 1 < n) cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+        return t;
+    }
+};
+
+}  // namespace
+
+}  // namespace gf
+
+using namespace gf;
+
+extern "C" {
+
+int gf_tree_build(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                  const float *pos4_dev, float theta2, int q5_asbuilt, gf_tree_info *info) {
+    clear_status();
+    if (!ctx || (n > 0 && (!pstart_dev || !pos4_dev)) || nhalo < 0) return GF_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    GF_TRY(build_tree(ctx, nhalo, n, pstart_dev, reinterpret_cast<const float4 *>(pos4_dev), theta2,
+                      q5_asbuilt, &ctx->last_tree));
+    if (info) {
+        info->nnode = ctx->last_tree.nnode;
+        info->nparticle = n;
+        info->nhalo = nhalo;
+    }
+    return check_device_errors(ctx);
+}
+
+int gf_tree_export(gf_ctx *ctx, void *bh_nodes, void *knn_nodes, float *pos4, int32_t *perm,
+                   int32_t *root, int32_t *rend) {
+    clear_status();
+    if (!ctx) return GF_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    return export_tree(ctx, ctx->last_tree, knn_nodes, bh_nodes, reinterpret_cast<float4 *>(pos4),
+                       perm, root, rend);
+}
+
+int gf_knn_density(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                   const float *pos4_dev, int k, int32_t *nearindex, float *dens) {
+    clear_status();
+    if (!ctx || (n > 0 && (!pstart_dev || !pos4_dev || !nearindex))) return GF_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    GF_TRY(build_tree(ctx, nhalo, n, pstart_dev, reinterpret_cast<const float4 *>(pos4_dev), 0.5f,
+                      0, &ctx->last_tree));
+    GF_TRY(launch_knn(ctx, ctx->last_tree, pstart_dev, k, nearindex, dens));
+    return check_device_errors(ctx);
+}
+
+int gf_self_potential(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                      const float *pos4_dev, float theta2, int32_t ndirect, double potentfact,
+                      int add_bg, float *penergy, float *raw) {
+    clear_status();
+    if (!ctx || (n > 0 && (!pstart_dev || !pos4_dev))) return GF_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    GF_TRY(build_tree(ctx, nhalo, n, pstart_dev, reinterpret_cast<const float4 *>(pos4_dev), theta2,
+                      0, &ctx->last_tree));
+    PotentialParams pp = potential_params(theta2, ndirect, potentfact, add_bg);
+    GF_TRY(launch_self_potential(ctx, ctx->last_tree, pstart_dev, pp, penergy, raw, nullptr));
+    return check_device_errors(ctx);
+}
+
+// ------------------------------------------------------------------ full stage
+int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *o,
+                 gf_stage_stats *st) {
+    clear_status();
+    if (!ctx || !b || !cfg || !o || b->nhalo < 0 || b->nparticle < 0) return GF_EINVAL;
+    if (b->nparticle > 0 && (!b->pstart || !b->x || !b->y || !b->z || !b->mass)) return GF_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    const int64_t n = b->nparticle;
+    const int32_t nh = b->nhalo;
+    cudaStream_t s = ctx->stream;
+    EventTimer tm(s, st != nullptr);
+    tm.mark();  // 0
+    // ---- 1. halo frames + FP64 recentring (Dump2BP / periodic unwrap)
+    GF_TRY(ctx->hid.reserve(sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    int32_t *hid = ctx->hid.as<int32_t>();
+    GF_TRY(compute_hid(ctx, nh, n, b->pstart, hid));
+    std::vector<double> frame, extent;
+    GF_TRY(halo_frames(ctx, b, hid, cfg->box, frame, extent));
+    const size_t nn = (size_t)std::max<int64_t>(n, 1);
+    const size_t dbytes = (nn * sizeof(double) + 255) & ~size_t(255);
+    GF_TRY(ctx->tmp[2].reserve(3 * dbytes + nn * sizeof(float4) + 256));
+    char *t2 = ctx->tmp[2].as<char>();
+    double *xr = o->xr ? o->xr : reinterpret_cast<double *>(t2);
+    double *yr = o->yr ? o->yr : reinterpret_cast<double *>(t2 + dbytes);
+    double *zr = o->zr ? o->zr : reinterpret_cast<double *>(t2 + 2 * dbytes);
+    float4 *pos = reinterpret_cast<float4 *>(t2 + 3 * dbytes);  // 256-byte aligned
+    // mesh plan from the recentred extents
+    std::vector<gf_mesh_desc> mesh((size_t)std::max(nh, 1));
+    int64_t cells = 0;
+    if (cfg->do_mesh) {
+        int sp = gf_plan_meshes(nh, extent.data(), &cfg->mesh, mesh.data(), &cells);
+        if (sp != GF_OK) return sp;
+    }
+    const size_t frame_bytes = frame.size() * sizeof(double);
+    const size_t mesh_bytes = mesh.size() * sizeof(gf_mesh_desc);
+    GF_TRY(ctx->mesh.reserve(frame_bytes + mesh_bytes + 512));
+    GF_TRY(ctx->pin[1].reserve(frame_bytes + mesh_bytes + 512));
+    memcpy(ctx->pin[1].ptr, frame.data(), frame_bytes);
+    memcpy(ctx->pin[1].as<char>() + ((frame_bytes + 255) & ~size_t(255)), mesh.data(), mesh_bytes);
+    GF_CUDA_TRY(cudaMemcpyAsync(ctx->mesh.ptr, ctx->pin[1].ptr,
+                                ((frame_bytes + 255) & ~size_t(255)) + mesh_bytes,
+                                cudaMemcpyHostToDevice, s));
+    const double *frame_dev = ctx->mesh.as<double>();
+    const gf_mesh_desc *mesh_dev =
+        reinterpret_cast<const gf_mesh_desc *>(ctx->mesh.as<char>() + ((frame_bytes + 255) & ~size_t(255)));
+    GF_TRY(recentre(ctx, b, hid, frame_dev, cfg->box, xr, yr, zr, pos));
+    tm.mark();  // 1
+    // ---- 2. octree
+    const bool need_tree = cfg->knn_k > 0 || cfg->do_potential;
+    if (need_tree)
+        GF_TRY(build_tree(ctx, nh, n, b->pstart, pos, cfg->theta2, cfg->q5_asbuilt, &ctx->last_tree));
+    tm.mark();  // 2
+    // ---- 3. kNN + SPH density
+    if (cfg->knn_k > 0) {
+        if (!o->nearindex) {
+            set_status(GF_EINVAL, "knn_k > 0 needs nearindex");
+            return GF_EINVAL;
+        }
+        GF_TRY(launch_knn(ctx, ctx->last_tree, b->pstart, cfg->knn_k, o->nearindex, o->dens_sph));
+    }
+    tm.mark();  // 3
+    // ---- 4. TSC mesh -> smoothing -> findDen
+    if (cfg->do_mesh) {
+        GF_TRY(ctx->tmp[3].reserve(sizeof(float) * (size_t)std::max<int64_t>(cells, 1)));
+        float *den = ctx->tmp[3].as<float>();
+        GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * cells, s));
+        const double vf = tsc_volfact();
+        GF_TRY(launch_tsc_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, mesh_dev, den, vf));
+        if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, cells, vf));
+        tm.mark();  // 4
+        GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den));
+        tm.mark();  // 5
+        if (o->dens_mesh) GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh));
+        tm.mark();  // 6
+    } else {
+        tm.mark();
+        tm.mark();
+        tm.mark();
+    }
+    // ---- 5. potential
+    unsigned long long *counters = nullptr;
+    if (cfg->do_potential) {
+        if (st) {
+            GF_TRY(ctx->tmp[4].reserve(64));
+            counters = ctx->tmp[4].as<unsigned long long>();
+            GF_CUDA_TRY(cudaMemsetAsync(counters, 0, 16, s));
+        }
+        const double pf = cfg->potentfact != 0.0 ? cfg->potentfact : physics().potentfact;
+        PotentialParams pp = potential_params(cfg->theta2, cfg->ndirect, pf, cfg->add_bg);
+        GF_TRY(launch_self_potential(ctx, ctx->last_tree, b->pstart, pp, o->penergy, nullptr, counters));
+    }
+    tm.mark();  // 7
+    int status = check_device_errors(ctx);
+    if (st) {
+        memset(st, 0, sizeof(*st));
+        st->nparticle = n;
+        st->nhalo = nh;
+        st->nnode = need_tree ? ctx->last_tree.nnode : 0;
+        st->mesh_cells = cells;
+        st->ms_recentre = tm.ms(0);
+        st->ms_tree = tm.ms(1);
+        st->ms_knn = tm.ms(2);
+        st->ms_tsc = tm.ms(3);
+        st->ms_smooth = tm.ms(4);
+        st->ms_findden = tm.ms(5);
+        st->ms_potential = tm.ms(6);
+        if (counters) {
+            unsigned long long hcnt[2] = {0, 0};
+            cudaMemcpy(hcnt, counters, 16, cudaMemcpyDeviceToHost);
+            st->pp_interactions = hcnt[0];
+            st->pc_interactions = hcnt[1];
+        }
+    }
+    return status;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ drop-ins
+namespace {
+
+int do_findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, int numnear,
+                      float *densph) {
+    if (np < 0 || (np > 0 && (!bp || !nearindex || !densph)) || numnear < 1 || numnear > 32) {
+        set_status(GF_EINVAL, "findsphdensity: invalid arguments (1 <= Numnear <= 32)");
+        return GF_EINVAL;
+    }
+    if (np == 0) return GF_OK;
+    gf_ctx *ctx = default_ctx();
+    if (!ctx) return last_status() ? last_status() : GF_EDEVICE;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    const size_t n = (size_t)np;
+    // stage x, y, z, mass (FP64) and pstart in one pinned buffer
+    const size_t hbytes = n * 4 * sizeof(double) + 2 * sizeof(int64_t);
+    GF_TRY(ctx->pin[0].reserve(hbytes));
+    GF_TRY(ctx->particles.reserve(hbytes + n * (sizeof(float4) + sizeof(int32_t) + sizeof(float)) + 1024));
+    GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    double *h = ctx->pin[0].as<double>();
+    for (size_t i = 0; i < n; i++) {
+        h[i] = bp[i].x;
+        h[n + i] = bp[i].y;
+        h[2 * n + i] = bp[i].z;
+        h[3 * n + i] = bp[i].mass;
+    }
+    int64_t *hp = reinterpret_cast<int64_t *>(h + 4 * n);
+    hp[0] = 0;
+    hp[1] = np;
+    char *d = ctx->particles.as<char>();
+    GF_CUDA_TRY(cudaMemcpyAsync(d, h, hbytes, cudaMemcpyHostToDevice, ctx->stream));
+    const double *dx = reinterpret_cast<const double *>(d);
+    const int64_t *dpstart = reinterpret_cast<const int64_t *>(dx + 4 * n);
+    float4 *pos = reinterpret_cast<float4 *>(d + ((hbytes + 255) & ~size_t(255)));
+    GF_TRY(ctx->tmp[1].reserve(n * (size_t)numnear * sizeof(int32_t) + n * sizeof(float) + 512));
+    int32_t *near32 = ctx->tmp[1].as<int32_t>();
+    float *dens = reinterpret_cast<float *>(near32 + n * numnear);
+    pack_pos_kernel<<<grid1(np), 256, 0, ctx->stream>>>(np, dx, dx + n, dx + 2 * n, nullptr, dx + 3 * n, pos);
+    GF_LAUNCH_CHECK();
+    GF_TRY(build_tree(ctx, 1, np, dpstart, pos, 0.5f, 0, &ctx->last_tree));
+    GF_TRY(launch_knn(ctx, ctx->last_tree, dpstart, numnear, near32, dens));
+    GF_TRY(ctx->pin[2].reserve(n * (size_t)numnear * sizeof(int32_t) + n * sizeof(float)));
+    int32_t *hn = ctx->pin[2].as<int32_t>();
+    GF_CUDA_TRY(cudaMemcpyAsync(hn, near32, n * (size_t)numnear * sizeof(int32_t) + n * sizeof(float),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+    GF_TRY(check_device_errors(ctx));  // synchronises
+    for (size_t i = 0; i < n * (size_t)numnear; i++) nearindex[i] = hn[i];
+    memcpy(densph, hn + n * numnear, n * sizeof(float));
+    return GF_OK;
+}
+
+int potent_common(int nend, Vector3d *r, float *penergy, int snp, Vector3d *sr, float *smass,
+                  bool self) {
+    gf_ctx *ctx = default_ctx();
+    if (!ctx) return last_status() ? last_status() : GF_EDEVICE;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    const size_t ns = (size_t)snp, nt = (size_t)nend;
+    // pinned staging: sources (3 doubles + mass), targets (3 doubles), pstart, target count
+    const size_t hbytes = ns * 3 * sizeof(double) + ns * sizeof(float) + (self ? 0 : nt * 3 * sizeof(double)) +
+                          4 * sizeof(int64_t);
+    GF_TRY(ctx->pin[0].reserve(hbytes + 64));
+    GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    char *h = ctx->pin[0].as<char>();
+    size_t off = 0;
+    memcpy(h + off, sr, ns * 3 * sizeof(double));
+    const size_t off_sr = off;
+    off += ns * 3 * sizeof(double);
+    memcpy(h + off, smass, ns * sizeof(float));
+    const size_t off_sm = off;
+    off += ns * sizeof(float);
+    off = (off + 7) & ~size_t(7);
+    const size_t off_tr = off;
+    if (!self) {
+        memcpy(h + off, r, nt * 3 * sizeof(double));
+        off += nt * 3 * sizeof(double);
+    }
+    const size_t off_ps = off;
+    int64_t *ps = reinterpret_cast<int64_t *>(h + off);
+    ps[0] = 0;
+    ps[1] = snp;
+    reinterpret_cast<int32_t *>(ps + 2)[0] = nend;  // target count of the single source halo
+    off += 4 * sizeof(int64_t);
+    const size_t dbytes = off + ns * sizeof(float4) + nt * (sizeof(float4) + sizeof(int32_t) + sizeof(float)) + 2048;
+    GF_TRY(ctx->particles.reserve(dbytes));
+    char *d = ctx->particles.as<char>();
+    GF_CUDA_TRY(cudaMemcpyAsync(d, h, off, cudaMemcpyHostToDevice, ctx->stream));
+    char *q = d + ((off + 255) & ~size_t(255));
+    float4 *spos = reinterpret_cast<float4 *>(q);
+    q += ((ns * sizeof(float4) + 255) & ~size_t(255));
+    float4 *tpos = reinterpret_cast<float4 *>(q);
+    q += ((nt * sizeof(float4) + 255) & ~size_t(255));
+    int32_t *thalo = reinterpret_cast<int32_t *>(q);
+    q += ((nt * sizeof(int32_t) + 255) & ~size_t(255));
+    float *dout = reinterpret_cast<float *>(q);
+    const int64_t *dps = reinterpret_cast<const int64_t *>(d + off_ps);
+    vec3_pos_kernel<<<grid1(snp), 256, 0, ctx->stream>>>(snp, reinterpret_cast<const double *>(d + off_sr),
+                                                         reinterpret_cast<const float *>(d + off_sm), spos);
+    GF_LAUNCH_CHECK();
+    const float theta2 = 0.5f;  // subhaloden.mod6.c:1481,1541
+    GF_TRY(build_tree(ctx, 1, snp, dps, spos, theta2, 0, &ctx->last_tree));
+    const gf_physics &ph = physics();
+    if (self) {
+        PotentialParams pp = potential_params(theta2, 100, ph.potentfact, 1);
+        GF_TRY(launch_self_potential(ctx, ctx->last_tree, dps, pp, dout, nullptr, nullptr));
+    } else {
+        // targets: FP32 positions, all looking into halo 0 (the one source tree);
+        // their masses do not enter the potential
+        GF_CUDA_TRY(cudaMemsetAsync(thalo, 0, nt * sizeof(int32_t), ctx->stream));
+        vec3_pos_kernel<<<grid1(nend), 256, 0, ctx->stream>>>(
+            nend, reinterpret_cast<const double *>(d + off_tr), nullptr, tpos);
+        GF_LAUNCH_CHECK();
+        // External_Halo_Potent sums directly below 1000 targets (subhaloden.mod6.c:1545)
+        PotentialParams pp = potential_params(theta2, 1000, ph.potentfact, 1);
+        const int32_t *ntarget_dev = reinterpret_cast<const int32_t *>(dps + 2);
+        GF_TRY(launch_external_potential(ctx, ctx->last_tree, dps, nend, tpos, thalo, ntarget_dev,
+                                         pp, dout, nullptr));
+    }
+    GF_CUDA_TRY(cudaMemcpyAsync(penergy, dout, nt * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    return check_device_errors(ctx);  // synchronises
+}
+
+}  // namespace
+
+extern "C" {
+
+void findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, int Numnear,
+                    float *densph) {
+    clear_status();
+    do_findsphdensity(bp, np, nearindex, Numnear, densph);
+}
+
+void Self_Halo_Potent(int np, Vector3d *r, float *mass, float *penergy) {
+    clear_status();
+    if (np < 0 || (np > 0 && (!r || !mass || !penergy))) {
+        set_status(GF_EINVAL, "Self_Halo_Potent: invalid arguments");
+        return;
+    }
+    if (np == 0) return;
+    potent_common(np, r, penergy, np, r, mass, true);
+}
+
+void External_Halo_Potent(int nend, Vector3d *r, float *mass, float *penergy, int snp,
+                          Vector3d *sr, float *smass) {
+    clear_status();
+    (void)mass;
+    if (nend < 0 || snp < 0 || (nend > 0 && (!r || !penergy)) || (snp > 0 && (!sr || !smass))) {
+        set_status(GF_EINVAL, "External_Halo_Potent: invalid arguments");
+        return;
+    }
+    if (nend == 0) return;
+    if (snp == 0) {  // no sources: only the background term of a zero mass
+        for (int i = 0; i < nend; i++) penergy[i] = 0.f;
+        return;
+    }
+    potent_common(nend, r, penergy, snp, sr, smass, false);
+}
+
+}  // extern "C"

@@ -165,6 +165,78 @@ int gf_gaussian_smooth(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host
 int gf_find_den(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh_dev, const float *den,
                 float *densph);
 
+/* ------------------------------------------------------------------------
+ * Centre-of-mass octree (ost.c:532-699 Make_Tree / divide_node, nnost.c:105-254
+ * new_Make_Tree_Near), kNN + SPH density (nnost.c:375-422 Find_Near,
+ * :560-630 findsphdensity) and Barnes-Hut potential (ost.c:226-251
+ * treeplumpotential; subhaloden.mod6.c:1477-1621) on device buffers.
+ * pos4: float4 (x, y, z, mass) per particle, recentred per halo; halo h is
+ * [pstart[h], pstart[h+1]).  Outputs are in input (batch) order.
+ * ---------------------------------------------------------------------- */
+typedef struct gf_tree_info {
+    int64_t nparticle;
+    int32_t nhalo;
+    int32_t nnode;
+} gf_tree_info;
+
+/* Builds the octree (kept in ctx until the next build). */
+int gf_tree_build(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                  const float *pos4_dev, float theta2, int q5_asbuilt, gf_tree_info *info);
+/* Copies the last tree to host memory: preorder potential nodes (80 bytes
+ * each), kNN nodes (40 bytes each), tree-ordered float4 positions, the
+ * tree-order -> batch-index permutation and each halo's preorder root/end.
+ * Any pointer may be NULL. */
+int gf_tree_export(gf_ctx *ctx, void *bh_nodes, void *knn_nodes, float *pos4, int32_t *perm,
+                   int32_t *root, int32_t *rend);
+/* k nearest neighbours (self included, k <= 32, ordered by distance then
+ * index; halo-local indices, -1 past a halo's size) and W4 density. */
+int gf_knn_density(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                   const float *pos4_dev, int k, int32_t *nearindex, float *dens);
+/* Self potential of every halo: penergy = phi * potentfact + bg(halo mass)
+ * (bg only if add_bg); halos with fewer than ndirect particles are summed
+ * directly.  raw (optional) receives phi itself. */
+int gf_self_potential(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                      const float *pos4_dev, float theta2, int32_t ndirect, double potentfact,
+                      int add_bg, float *penergy, float *raw);
+
+/* ------------------------------------------------------------------------
+ * The whole per-halo stage on a batch: FP64 recentring (Dump2BP) with
+ * periodic unwrap, octree, kNN + SPH density, TSC mesh + smoothing + findDen,
+ * and the self potential of every halo.
+ * ---------------------------------------------------------------------- */
+typedef struct gf_stage_config {
+    gf_mesh_rule mesh;
+    double box;            /* periodic box size, cMpc/h (0: no unwrap) */
+    int32_t knn_k;         /* neighbours per particle incl. self (0: skip kNN) */
+    int32_t do_mesh;       /* TSC + smoothing + findDen */
+    int32_t do_potential;  /* tree potential */
+    int32_t ndirect;       /* direct-sum threshold (Self_Halo_Potent: 100) */
+    float theta2;          /* opening parameter (0.5 in the reference) */
+    int32_t add_bg;        /* add GetBGpotent of each halo's mass */
+    int32_t q5_asbuilt;    /* reproduce ost.c:571's y*x in place of y*z */
+    int32_t reserved;
+    double potentfact;     /* 0: from gf_get_physics() */
+} gf_stage_config;
+
+typedef struct gf_stage_out {
+    int32_t *nearindex;    /* device, n*knn_k halo-local indices */
+    float *dens_sph;       /* device, n (may be NULL) */
+    float *dens_mesh;      /* device, n (may be NULL) */
+    float *penergy;        /* device, n (may be NULL) */
+    double *xr, *yr, *zr;  /* device, n recentred positions (may be NULL) */
+} gf_stage_out;
+
+typedef struct gf_stage_stats {
+    int64_t nparticle, nnode, mesh_cells;
+    int32_t nhalo, reserved;
+    uint64_t pp_interactions, pc_interactions;
+    float ms_recentre, ms_tree, ms_knn, ms_tsc, ms_smooth, ms_findden, ms_potential, ms_pad;
+} gf_stage_stats;
+
+/* stats may be NULL; when given, per-phase CUDA-event times are filled in. */
+int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *out,
+                 gf_stage_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -364,3 +364,95 @@ int or_sph_density(int64_t np, int k, const double *d2, float *dens) {
     }
     return 0;
 }
+
+/* ---------------------------------------------------------------- potential */
+/* Node record exported by libgf (gf_tree_export), preorder. */
+typedef struct {
+    double com[3];
+    double open_r2;
+    float mass, trq;
+    float q[6];
+    int32_t skip, lstart, lcount, count;
+} or_bhnode;
+
+/* FP64 evaluation of the walk of ost.c:226-251 on a given tree: the same
+ * opening decisions as the tree's owner (|t - com|^2 < open_r2 evaluated
+ * with the same separately rounded double operations), exact terms -m/r for
+ * opened loose particles, and for accepted cells the monopole + quadrupole
+ * expansion about the node's exported centre with mass and second moments
+ * recomputed in FP64 from the node's particles.  (Cell term of
+ * CELLPLUMPOTENT, ost.c:144-176, with exact kernels in place of the spline
+ * tables.) */
+int or_tree_potential(int32_t nnode, const void *nodes_v, int64_t nsrc, const float *sx,
+                      const float *sy, const float *sz, const float *sm, int64_t ntgt,
+                      const float *tx, const float *ty, const float *tz, const int32_t *troot,
+                      const int32_t *trend, const int32_t *topen, double *phi) {
+    const or_bhnode *nodes = (const or_bhnode *)nodes_v;
+    double *M = (double *)malloc(sizeof(double) * (nnode > 0 ? nnode : 1));
+    double *Q = (double *)malloc(sizeof(double) * 6 * (nnode > 0 ? nnode : 1));
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int32_t i = 0; i < nnode; i++) {
+        const or_bhnode *nd = nodes + i;
+        double m = 0, q[6] = {0, 0, 0, 0, 0, 0};
+        for (int64_t j = nd->lstart; j < (int64_t)nd->lstart + nd->count; j++) {
+            double dx = (double)sx[j] - nd->com[0], dy = (double)sy[j] - nd->com[1],
+                   dz = (double)sz[j] - nd->com[2], w = sm[j];
+            m += w;
+            q[0] += w * dx * dx; q[1] += w * dy * dy; q[2] += w * dz * dz;
+            q[3] += w * dx * dy; q[4] += w * dx * dz; q[5] += w * dy * dz;
+        }
+        M[i] = m;
+        for (int a = 0; a < 6; a++) Q[6 * (int64_t)i + a] = q[a];
+    }
+    (void)nsrc;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t t = 0; t < ntgt; t++) {
+        const double px = (double)tx[t], py = (double)ty[t], pz = (double)tz[t];
+        double acc = 0.0;
+        int32_t i = troot[t];
+        const int32_t end = trend[t];
+        while (i < end) {
+            const or_bhnode *nd = nodes + i;
+            const double dx = px - nd->com[0], dy = py - nd->com[1], dz = pz - nd->com[2];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if ((topen && topen[t]) || d2 < nd->open_r2) {
+                for (int64_t j = nd->lstart; j < (int64_t)nd->lstart + nd->lcount; j++) {
+                    double ex = px - sx[j], ey = py - sy[j], ez = pz - sz[j];
+                    double r2 = ex * ex + ey * ey + ez * ez;
+                    if (r2 > 0) acc += -(double)sm[j] / sqrt(r2);
+                }
+                i = i + 1;
+            } else {
+                const double *q = Q + 6 * (int64_t)i;
+                const double r = sqrt(d2);
+                const double qxy = q[0] * dx * dx + q[1] * dy * dy + q[2] * dz * dz +
+                                   2. * (q[3] * dx * dy + q[4] * dx * dz + q[5] * dy * dz);
+                acc += -M[i] / r + 0.5 * (q[0] + q[1] + q[2]) / (r * r * r) -
+                       1.5 * qxy / (r * r * r * r * r);
+                i = nd->skip;
+            }
+        }
+        phi[t] = acc;
+    }
+    free(Q);
+    free(M);
+    return 0;
+}
+
+/* FP64 direct sum: phi_t = sum over sources at nonzero distance of -m/r. */
+int or_direct_potential(int64_t nsrc, const float *sx, const float *sy, const float *sz,
+                        const float *sm, int64_t ntgt, const float *tx, const float *ty,
+                        const float *tz, double *phi) {
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < ntgt; t++) {
+        double acc = 0.0;
+        const double px = tx[t], py = ty[t], pz = tz[t];
+        for (int64_t j = 0; j < nsrc; j++) {
+            double ex = px - sx[j], ey = py - sy[j], ez = pz - sz[j];
+            double r2 = ex * ex + ey * ey + ez * ez;
+            if (r2 > 0) acc += -(double)sm[j] / sqrt(r2);
+        }
+        phi[t] = acc;
+    }
+    return 0;
+}

@@ -44,4 +44,19 @@ int or_knn_grid(int64_t np, const float *x, const float *y, const float *z, int 
  * arithmetic (W4: nnost.c:536-555). */
 int or_sph_density(int64_t np, int k, const double *d2, float *dens);
 
+
+
+/* FP64 walk of a tree exported by libgf (same opening decisions, exact
+ * terms): ost.c:72-83 (treeopen), :144-193 (cell/particle terms), :226-251.
+ * nodes: preorder records of gf_tree_export (80 bytes each); sources in tree
+ * order; topen[t] != 0 opens every node (direct sum). */
+int or_tree_potential(int32_t nnode, const void *nodes, int64_t nsrc, const float *sx,
+                      const float *sy, const float *sz, const float *sm, int64_t ntgt,
+                      const float *tx, const float *ty, const float *tz, const int32_t *troot,
+                      const int32_t *trend, const int32_t *topen, double *phi);
+
+/* FP64 direct-sum potential (subhaloden.mod6.c:1493-1503 in double). */
+int or_direct_potential(int64_t nsrc, const float *sx, const float *sy, const float *sz,
+                        const float *sm, int64_t ntgt, const float *tx, const float *ty,
+                        const float *tz, double *phi);
 #endif

@@ -52,6 +52,9 @@ class Restatement:
             L.or_knn_brute.argtypes = [_I64, _VP, _VP, _VP, _I, _VP, _VP]
             L.or_knn_grid.argtypes = [_I64, _VP, _VP, _VP, _I, _VP, _VP]
             L.or_sph_density.argtypes = [_I64, _I, _VP, _VP]
+            L.or_tree_potential.argtypes = [ctypes.c_int32, _VP, _I64, _VP, _VP, _VP, _VP, _I64,
+                                            _VP, _VP, _VP, _VP, _VP, _VP, _VP]
+            L.or_direct_potential.argtypes = [_I64, _VP, _VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP]
             Restatement._lib = L
         self.L = Restatement._lib
 
@@ -102,6 +105,34 @@ class Restatement:
         out = np.zeros(n, np.float32)
         self.L.or_sph_density(n, k, _p(d2), _p(out))
         return out
+
+
+    def tree_potential(self, nodes, spos4, tpos, troot, trend, topen=None):
+        """FP64 walk of an exported tree.  nodes: BH_NODE_DTYPE array;
+        spos4: (n, 4) float32 tree-ordered sources; tpos: (m, 3) float32."""
+        nodes = np.ascontiguousarray(nodes)
+        s = np.ascontiguousarray(spos4, np.float32)
+        sx, sy, sz, sm = (np.ascontiguousarray(s[:, i]) for i in range(4))
+        t = np.ascontiguousarray(tpos, np.float32)
+        tx, ty, tz = (np.ascontiguousarray(t[:, i]) for i in range(3))
+        troot = np.ascontiguousarray(troot, np.int32)
+        trend = np.ascontiguousarray(trend, np.int32)
+        to = None if topen is None else np.ascontiguousarray(topen, np.int32)
+        phi = np.zeros(len(t), np.float64)
+        self.L.or_tree_potential(len(nodes), _p(nodes), len(s), _p(sx), _p(sy), _p(sz), _p(sm),
+                                 len(t), _p(tx), _p(ty), _p(tz), _p(troot), _p(trend), _p(to),
+                                 _p(phi))
+        return phi
+
+    def direct_potential(self, spos4, tpos):
+        s = np.ascontiguousarray(spos4, np.float32)
+        sx, sy, sz, sm = (np.ascontiguousarray(s[:, i]) for i in range(4))
+        t = np.ascontiguousarray(tpos, np.float32)
+        tx, ty, tz = (np.ascontiguousarray(t[:, i]) for i in range(3))
+        phi = np.zeros(len(t), np.float64)
+        self.L.or_direct_potential(len(s), _p(sx), _p(sy), _p(sz), _p(sm), len(t), _p(tx), _p(ty),
+                                   _p(tz), _p(phi))
+        return phi
 
 
 class Reference:
