@@ -36,21 +36,32 @@ struct SmoothTile {
     int32_t npen;   // pencils in this tile
 };
 
-// Tile b of one axis pass -> (halo, pencil range).  tile_start holds the
-// per-halo prefix of tile counts for that axis (nhalo+1 entries).
+struct AxisTable {
+    int32_t n;
+    int32_t logn;     // log2(n) for the FFT path, -1 for the direct path
+    int64_t tab_off;  // float offset of this axis' tables
+};
+
+struct GroupLaunch {
+    const int32_t *halos;      // halos of this (axis, length) group
+    const int64_t *tile_start; // prefix of tile counts over the group (ngroup + 1)
+    int32_t ngroup;
+};
+
 template <int AXIS>
-__device__ __forceinline__ SmoothTile decode_tile(int64_t b, const int64_t *__restrict__ tile_start,
-                                                  int nhalo, const gf_mesh_desc *__restrict__ mesh,
-                                                  int pmax) {
-    int lo = 0, hi = nhalo;  // largest h with tile_start[h] <= b
+__device__ __forceinline__ SmoothTile decode_group_tile(int64_t b, const GroupLaunch &g,
+                                                        const gf_mesh_desc *__restrict__ mesh,
+                                                        int pmax) {
+    int lo = 0, hi = g.ngroup;
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
-        if (tile_start[mid] <= b) lo = mid; else hi = mid;
+        if (g.tile_start[mid] <= b) lo = mid; else hi = mid;
     }
-    const int64_t local = b - tile_start[lo];
-    const gf_mesh_desc &m = mesh[lo];
+    const int64_t local = b - g.tile_start[lo];
+    const int h = g.halos[lo];
+    const gf_mesh_desc &m = mesh[h];
     SmoothTile t;
-    t.halo = lo;
+    t.halo = h;
     if (AXIS == 0) {
         const int rows = m.ny * m.nz;
         t.base = (int)(local * pmax);
@@ -65,12 +76,6 @@ __device__ __forceinline__ SmoothTile decode_tile(int64_t b, const int64_t *__re
     return t;
 }
 
-struct AxisTable {
-    int32_t n;
-    int32_t logn;     // log2(n) for the FFT path, -1 for the direct path
-    int64_t tab_off;  // float offset of this axis' tables
-};
-
 constexpr int kThreads = 256;
 
 template <int AXIS>
@@ -84,10 +89,10 @@ __device__ __forceinline__ int64_t elem_addr(const gf_mesh_desc &m, int64_t mx, 
 template <int AXIS>
 __global__ void __launch_bounds__(kThreads)
 smooth_axis_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh,
-                   const int64_t *__restrict__ tile_start, int nhalo,
-                   const AxisTable *__restrict__ axes, const float *__restrict__ tables, int pmax) {
+                   GroupLaunch g, const AxisTable *__restrict__ axes,
+                   const float *__restrict__ tables, int pmax) {
     extern __shared__ float2 smem[];
-    const SmoothTile t = decode_tile<AXIS>(blockIdx.x, tile_start, nhalo, mesh, pmax);
+    const SmoothTile t = decode_group_tile<AXIS>(blockIdx.x, g, mesh, pmax);
     const gf_mesh_desc m = mesh[t.halo];
     const AxisTable at = axes[3 * t.halo + AXIS];
     const int n = at.n;
@@ -180,6 +185,162 @@ smooth_axis_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mes
     }
 }
 
+// ---------------------------------------------------------------- FFT path
+// In-register R-point DFT (R = 2, 4, 8) of a[], forward e^{-2 pi i jk/R} or
+// inverse (conjugate) kernel.
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 v) {  // v * (-i) forward, v * (+i) inverse
+    return INV ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2 &a0, float2 &a1, float2 &a2, float2 &a3) {
+    const float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3);
+    const float2 t3 = mul_mi<INV>(csub(a1, a3));
+    a0 = cadd(t0, t2);
+    a2 = csub(t0, t2);
+    a1 = cadd(t1, t3);
+    a3 = csub(t1, t3);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 (&a)[R]) {
+    if (R == 2) {
+        const float2 t = a[0];
+        a[0] = cadd(t, a[1]);
+        a[1] = csub(t, a[1]);
+    } else if (R == 4) {
+        dft4<INV>(a[0], a[1], a[2], a[3]);
+    } else {  // R == 8: two 4-point DFTs (even, odd) and the W8 butterflies
+        float2 e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
+        float2 o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+        dft4<INV>(e0, e1, e2, e3);
+        dft4<INV>(o0, o1, o2, o3);
+        const float h = 0.70710678118654752f;
+        // W8^1 = (1 - i)/sqrt2 forward, (1 + i)/sqrt2 inverse; W8^2 = -/+ i; W8^3 = (-1 -/+ i)/sqrt2
+        o1 = INV ? make_float2(h * (o1.x - o1.y), h * (o1.x + o1.y))
+                 : make_float2(h * (o1.x + o1.y), h * (o1.y - o1.x));
+        o2 = mul_mi<INV>(o2);
+        o3 = INV ? make_float2(-h * (o3.x + o3.y), h * (o3.x - o3.y))
+                 : make_float2(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+        a[0] = cadd(e0, o0); a[4] = csub(e0, o0);
+        a[1] = cadd(e1, o1); a[5] = csub(e1, o1);
+        a[2] = cadd(e2, o2); a[6] = csub(e2, o2);
+        a[3] = cadd(e3, o3); a[7] = csub(e3, o3);
+    }
+}
+
+// One Stockham radix-R pass over NP complex pencils of length N held in
+// shared memory (src -> dst), stride S = product of the radices already done:
+//   y[q + S (R p + j)] = w^(p S j) * sum_r x[q + S (p + r M)] e^{-+2 pi i r j/R},
+// M = N/(S R), w = e^{-2 pi i/N} (table tw, conjugated for the inverse).  The
+// final pass of the forward transform multiplies by the filter.
+template <int N, int R, int S, bool INV, bool FILTER>
+__device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                              int npair, const float2 *__restrict__ tw,
+                                              const float *__restrict__ filt) {
+    constexpr int M = N / (S * R);
+    constexpr int ITEMS = N / R;  // butterflies per pencil
+    for (int e = threadIdx.x; e < npair * ITEMS; e += blockDim.x) {
+        const int c = e / ITEMS;  // ITEMS is a power of two
+        const int t = e - c * ITEMS;
+        const int q = t % S;
+        const int p = t / S;
+        const float2 *x = src + c * N;
+        float2 *y = dst + c * N;
+        float2 a[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) a[r] = x[q + S * (p + r * M)];
+        dft<R, INV>(a);
+#pragma unroll
+        for (int j = 1; j < R; j++) {
+            float2 w = tw[(p * S * j) & (N - 1)];
+            if (INV) w.y = -w.y;
+            a[j] = cmul(a[j], w);
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const int k = q + S * (R * p + j);
+            float2 v = a[j];
+            if (FILTER) {
+                const float g = filt[k];
+                v.x *= g;
+                v.y *= g;
+            }
+            y[k] = v;
+        }
+    }
+    __syncthreads();
+}
+
+// Forward FFT, filter, inverse FFT of every pencil pair; result in buf[0].
+template <int LOGN>
+__device__ __forceinline__ void fft_filter_ifft(float2 *b0, float2 *b1, int npair, const float2 *tw,
+                                                const float *filt) {
+    constexpr int N = 1 << LOGN;
+    // radix plan: 8, 8, then 1 (LOGN 6), 2 (7), 4 (8), 8 (9)
+    constexpr int R3 = LOGN == 6 ? 1 : LOGN == 7 ? 2 : LOGN == 8 ? 4 : 8;
+    static_assert(LOGN >= 6 && LOGN <= 9, "FFT lengths 64..512");
+    if (R3 == 1) {
+        stockham_pass<N, 8, 1, false, false>(b0, b1, npair, tw, filt);
+        stockham_pass<N, 8, 8, false, true>(b1, b0, npair, tw, filt);
+        stockham_pass<N, 8, 1, true, false>(b0, b1, npair, tw, filt);
+        stockham_pass<N, 8, 8, true, false>(b1, b0, npair, tw, filt);
+    } else {
+        constexpr int R3v = R3 == 1 ? 2 : R3;
+        stockham_pass<N, 8, 1, false, false>(b0, b1, npair, tw, filt);
+        stockham_pass<N, 8, 8, false, false>(b1, b0, npair, tw, filt);
+        stockham_pass<N, R3v, 64, false, true>(b0, b1, npair, tw, filt);
+        stockham_pass<N, 8, 1, true, false>(b1, b0, npair, tw, filt);
+        stockham_pass<N, 8, 8, true, false>(b0, b1, npair, tw, filt);
+        stockham_pass<N, R3v, 64, true, false>(b1, b0, npair, tw, filt);
+    }
+}
+
+constexpr int kPencils = 32;  // real pencils per FFT tile (16 complex)
+
+template <int AXIS, int LOGN>
+__global__ void __launch_bounds__((kPencils / 2) * (1 << LOGN) / 8)
+smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh, GroupLaunch g,
+                  const AxisTable *__restrict__ axes, const float *__restrict__ tables) {
+    constexpr int N = 1 << LOGN;
+    extern __shared__ float2 smem[];
+    const SmoothTile t = decode_group_tile<AXIS>(blockIdx.x, g, mesh, kPencils);
+    const gf_mesh_desc m = mesh[t.halo];
+    const AxisTable at = axes[3 * t.halo + AXIS];
+    const int64_t mx = 2 * (m.nx / 2 + 1);
+    const int npair = (t.npen + 1) >> 1;
+    float2 *b0 = smem;
+    float2 *b1 = smem + (kPencils / 2) * N;
+    float *fa = reinterpret_cast<float *>(b0);
+    const int total = 2 * npair * N;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        int p, s;
+        if (AXIS == 0) { p = e >> LOGN; s = e & (N - 1); }
+        else { s = e / (2 * npair); p = e - s * (2 * npair); }
+        float v = 0.f;
+        if (p < t.npen) v = den[elem_addr<AXIS>(m, mx, t, p, s)];
+        fa[2 * ((p >> 1) * N + s) + (p & 1)] = v;
+    }
+    __syncthreads();
+    // full twiddle table e^{-2 pi i k/N}, k < N, then N filter factors G/N
+    const float2 *tw = reinterpret_cast<const float2 *>(tables + at.tab_off);
+    const float *filt = tables + at.tab_off + 2 * N;
+    fft_filter_ifft<LOGN>(b0, b1, npair, tw, filt);
+    const float *fs = reinterpret_cast<const float *>(b0);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        int p, s;
+        if (AXIS == 0) { p = e >> LOGN; s = e & (N - 1); }
+        else { s = e / (2 * npair); p = e - s * (2 * npair); }
+        if (p < t.npen) den[elem_addr<AXIS>(m, mx, t, p, s)] = fs[2 * ((p >> 1) * N + s) + (p & 1)];
+    }
+}
+
 int ilog2_exact(int n) {
     if (n <= 0 || (n & (n - 1))) return -1;
     int l = 0;
@@ -196,12 +357,26 @@ double axis_factor(int k, int n, double rg_cells) {
     return exp((double)(ks * ks) * expfac / ((double)n * (double)n));
 }
 
+enum PathKind { PATH_FFT8 = 0, PATH_RADIX2 = 1, PATH_DIRECT = 2 };
+
+PathKind path_of(int n) {
+    const int l = ilog2_exact(n);
+    if (l >= 6 && l <= 9) return PATH_FFT8;
+    if (l >= 1) return PATH_RADIX2;
+    return PATH_DIRECT;
+}
+
+// Table layouts: FFT8: [e^{-2 pi i k/n}, k < n (float2)][G/n (n floats)];
+// RADIX2: [e^{-2 pi i k/n}, k < n/2 (float2)][G/n]; DIRECT: [h_n (n floats)].
+// Twiddles and filters are evaluated in FP64 and rounded once.
 void append_tables(std::vector<float> &tab, int n, double rg_cells, AxisTable &at) {
+    const PathKind pk = path_of(n);
     at.n = n;
-    at.logn = ilog2_exact(n);
+    at.logn = pk == PATH_DIRECT ? -1 : ilog2_exact(n);
     at.tab_off = (int64_t)tab.size();
-    if (at.logn >= 0) {
-        for (int k = 0; k < n / 2; k++) {  // forward twiddles e^{-2 pi i k/n}
+    if (pk != PATH_DIRECT) {
+        const int ntw = pk == PATH_FFT8 ? n : n / 2;
+        for (int k = 0; k < ntw; k++) {
             const double ang = 2.0 * M_PI * (double)k / (double)n;
             tab.push_back((float)cos(ang));
             tab.push_back((float)-sin(ang));
@@ -221,20 +396,40 @@ void append_tables(std::vector<float> &tab, int n, double rg_cells, AxisTable &a
     }
 }
 
+template <int AXIS, int LOGN>
+int launch_fft(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunch g, int64_t ntiles,
+               const AxisTable *axes, const float *tables) {
+    constexpr int N = 1 << LOGN;
+    const int threads = (kPencils / 2) * N / 8;
+    const size_t smem = (size_t)2 * (kPencils / 2) * N * sizeof(float2);
+    GF_CUDA_TRY(cudaFuncSetAttribute(smooth_fft_kernel<AXIS, LOGN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    smooth_fft_kernel<AXIS, LOGN><<<(unsigned)ntiles, threads, smem, ctx->stream>>>(den, mesh_dev, g,
+                                                                                   axes, tables);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
 template <int AXIS>
-int launch_axis(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, const int64_t *tile_start,
-                int nhalo, int64_t ntiles, const AxisTable *axes, const float *tables, int pmax,
-                int nmax) {
+int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunch g,
+                 int64_t ntiles, int n, int pmax, const AxisTable *axes, const float *tables) {
     if (ntiles == 0) return GF_OK;
     if (ntiles > 0x7fffffffLL) {
         set_status(GF_ENOTIMPL, "%lld smoothing tiles exceed one launch", (long long)ntiles);
         return GF_ENOTIMPL;
     }
-    const size_t smem = (size_t)2 * ((pmax + 1) / 2) * nmax * sizeof(float2);
+    switch (path_of(n) == PATH_FFT8 ? ilog2_exact(n) : 0) {
+        case 6: return launch_fft<AXIS, 6>(ctx, den, mesh_dev, g, ntiles, axes, tables);
+        case 7: return launch_fft<AXIS, 7>(ctx, den, mesh_dev, g, ntiles, axes, tables);
+        case 8: return launch_fft<AXIS, 8>(ctx, den, mesh_dev, g, ntiles, axes, tables);
+        case 9: return launch_fft<AXIS, 9>(ctx, den, mesh_dev, g, ntiles, axes, tables);
+        default: break;
+    }
+    const size_t smem = (size_t)2 * ((pmax + 1) / 2) * n * sizeof(float2);
     GF_CUDA_TRY(cudaFuncSetAttribute(smooth_axis_kernel<AXIS>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    smooth_axis_kernel<AXIS><<<(unsigned)ntiles, kThreads, smem, ctx->stream>>>(
-        den, mesh_dev, tile_start, nhalo, axes, tables, pmax);
+    smooth_axis_kernel<AXIS><<<(unsigned)ntiles, kThreads, smem, ctx->stream>>>(den, mesh_dev, g, axes,
+                                                                                tables, pmax);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }
@@ -247,7 +442,6 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
     std::vector<AxisTable> axes(3 * (size_t)nhalo);
     std::vector<float> tables;
     std::map<std::pair<int, double>, AxisTable> cache;
-    int nmax = 0;
     for (int h = 0; h < nhalo; h++) {
         const gf_mesh_desc &m = mesh_host[h];
         if (m.nx < 1 || m.ny < 1 || m.nz < 1 || !(m.cellsize > 0)) {
@@ -266,34 +460,66 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
                 it = cache.emplace(key, at).first;
             }
             axes[3 * (size_t)h + a] = it->second;
-            if (dims[a] > nmax) nmax = dims[a];
         }
     }
-    // pencils per tile: 32 (a full 128-byte row of a y/z tile) unless the
-    // ping-pong buffers would exceed the shared memory of one block
-    int pmax = 32;
-    while (pmax > 2 && (size_t)2 * (pmax / 2) * nmax * sizeof(float2) > 200 * 1024) pmax -= 2;
-    if ((size_t)2 * (pmax / 2) * nmax * sizeof(float2) > 200 * 1024) {
-        set_status(GF_ENOTIMPL, "mesh axis of %d cells exceeds the shared-memory pencil tile", nmax);
-        return GF_ENOTIMPL;
+    // groups: (axis, n) for the FFT path; one group per axis for the rest
+    struct Group {
+        int axis, n, pmax;
+        std::vector<int32_t> halos;
+        std::vector<int64_t> start;
+    };
+    std::vector<Group> groups;
+    std::map<std::pair<int, int>, size_t> gidx;
+    for (int a = 0; a < 3; a++) {
+        for (int h = 0; h < nhalo; h++) {
+            const gf_mesh_desc &m = mesh_host[h];
+            const int dims[3] = {m.nx, m.ny, m.nz};
+            const int n = dims[a];
+            const int key_n = path_of(n) == PATH_FFT8 ? n : -1;
+            auto k = std::make_pair(a, key_n);
+            auto it = gidx.find(k);
+            if (it == gidx.end()) {
+                it = gidx.emplace(k, groups.size()).first;
+                groups.push_back(Group{a, n, 0, {}, {0}});
+            }
+            Group &g = groups[it->second];
+            g.halos.push_back(h);
+            g.n = std::max(g.n, n);
+        }
     }
-    std::vector<int64_t> tstart[3];
-    for (int a = 0; a < 3; a++) tstart[a].assign((size_t)nhalo + 1, 0);
-    for (int h = 0; h < nhalo; h++) {
-        const gf_mesh_desc &m = mesh_host[h];
-        const int64_t cx = (m.nx + pmax - 1) / pmax;
-        tstart[0][h + 1] = tstart[0][h] + ((int64_t)m.ny * m.nz + pmax - 1) / pmax;
-        tstart[1][h + 1] = tstart[1][h] + cx * m.nz;
-        tstart[2][h + 1] = tstart[2][h] + cx * m.ny;
+    for (Group &g : groups) {
+        if (path_of(g.n) == PATH_FFT8 && g.n == (1 << ilog2_exact(g.n))) {
+            g.pmax = kPencils;
+        } else {
+            int pmax = 32;
+            while (pmax > 2 && (size_t)2 * (pmax / 2) * g.n * sizeof(float2) > 200 * 1024) pmax -= 2;
+            if ((size_t)2 * (pmax / 2) * g.n * sizeof(float2) > 200 * 1024) {
+                set_status(GF_ENOTIMPL, "mesh axis of %d cells exceeds the shared-memory pencil tile", g.n);
+                return GF_ENOTIMPL;
+            }
+            g.pmax = pmax;
+        }
+        for (int32_t h : g.halos) {
+            const gf_mesh_desc &m = mesh_host[h];
+            const int64_t cx = (m.nx + g.pmax - 1) / g.pmax;
+            int64_t c = g.axis == 0 ? ((int64_t)m.ny * m.nz + g.pmax - 1) / g.pmax
+                                    : cx * (g.axis == 1 ? m.nz : m.ny);
+            g.start.push_back(g.start.back() + c);
+        }
     }
-    // stage everything in one device buffer: [axes | tables | starts x | starts y | starts z]
+    // one staging buffer: [axes | tables | per group: halos, starts]
     auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
-    const size_t off_tab = align(axes.size() * sizeof(AxisTable));
-    const size_t off_s0 = align(off_tab + tables.size() * sizeof(float));
-    const size_t sbytes = ((size_t)nhalo + 1) * sizeof(int64_t);
-    const size_t off_s1 = align(off_s0 + sbytes);
-    const size_t off_s2 = align(off_s1 + sbytes);
-    const size_t total = off_s2 + sbytes;
+    size_t off = align(axes.size() * sizeof(AxisTable));
+    const size_t off_tab = off;
+    off = align(off + tables.size() * sizeof(float));
+    std::vector<size_t> off_h(groups.size()), off_s(groups.size());
+    for (size_t i = 0; i < groups.size(); i++) {
+        off_h[i] = off;
+        off = align(off + groups[i].halos.size() * sizeof(int32_t));
+        off_s[i] = off;
+        off = align(off + groups[i].start.size() * sizeof(int64_t));
+    }
+    const size_t total = off;
     GF_TRY(ctx->smooth_tables.reserve(total));
     GF_TRY(ctx->pin[3].reserve(total));
     char *hbuf = ctx->pin[3].as<char>();
@@ -301,19 +527,25 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
     GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     memcpy(hbuf, axes.data(), axes.size() * sizeof(AxisTable));
     memcpy(hbuf + off_tab, tables.data(), tables.size() * sizeof(float));
-    memcpy(hbuf + off_s0, tstart[0].data(), sbytes);
-    memcpy(hbuf + off_s1, tstart[1].data(), sbytes);
-    memcpy(hbuf + off_s2, tstart[2].data(), sbytes);
+    for (size_t i = 0; i < groups.size(); i++) {
+        memcpy(hbuf + off_h[i], groups[i].halos.data(), groups[i].halos.size() * sizeof(int32_t));
+        memcpy(hbuf + off_s[i], groups[i].start.data(), groups[i].start.size() * sizeof(int64_t));
+    }
     char *dbuf = ctx->smooth_tables.as<char>();
     GF_CUDA_TRY(cudaMemcpyAsync(dbuf, hbuf, total, cudaMemcpyHostToDevice, ctx->stream));
     const AxisTable *d_axes = reinterpret_cast<const AxisTable *>(dbuf);
     const float *d_tab = reinterpret_cast<const float *>(dbuf + off_tab);
-    GF_TRY(launch_axis<0>(ctx, den, mesh_dev, reinterpret_cast<const int64_t *>(dbuf + off_s0),
-                          nhalo, tstart[0][nhalo], d_axes, d_tab, pmax, nmax));
-    GF_TRY(launch_axis<1>(ctx, den, mesh_dev, reinterpret_cast<const int64_t *>(dbuf + off_s1),
-                          nhalo, tstart[1][nhalo], d_axes, d_tab, pmax, nmax));
-    GF_TRY(launch_axis<2>(ctx, den, mesh_dev, reinterpret_cast<const int64_t *>(dbuf + off_s2),
-                          nhalo, tstart[2][nhalo], d_axes, d_tab, pmax, nmax));
+    for (size_t i = 0; i < groups.size(); i++) {
+        const Group &g = groups[i];
+        GroupLaunch gl;
+        gl.halos = reinterpret_cast<const int32_t *>(dbuf + off_h[i]);
+        gl.tile_start = reinterpret_cast<const int64_t *>(dbuf + off_s[i]);
+        gl.ngroup = (int32_t)g.halos.size();
+        const int64_t nt = g.start.back();
+        if (g.axis == 0) GF_TRY(launch_group<0>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
+        else if (g.axis == 1) GF_TRY(launch_group<1>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
+        else GF_TRY(launch_group<2>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
+    }
     return GF_OK;
 }
 
