@@ -371,6 +371,9 @@ PathKind path_of(int n) {
 // Twiddles and filters are evaluated in FP64 and rounded once.
 void append_tables(std::vector<float> &tab, int n, double rg_cells, AxisTable &at) {
     const PathKind pk = path_of(n);
+    // every table starts on a 16-byte boundary: the FFT paths read float2
+    // twiddles, and a preceding table may hold an odd number of floats
+    while (tab.size() % 4) tab.push_back(0.f);
     at.n = n;
     at.logn = pk == PATH_DIRECT ? -1 : ilog2_exact(n);
     at.tab_off = (int64_t)tab.size();

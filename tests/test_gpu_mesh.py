@@ -153,3 +153,19 @@ def test_smoothing_every_fft_length_vs_fp64(restatement, cuda_device, dims):
     dropin.gaussian_Smoothing(got, nx, ny, nz, 0.004, 0.008)
     a, b = _logical(got, nx, ny, nz), _logical(exact, nx, ny, nz)
     assert np.abs(a - b).max() / np.abs(b).max() < 2e-6
+
+
+def test_smoothing_odd_direct_axis_before_fft_axes(restatement, cuda_device):
+    """A 37-cell (direct convolution) axis ahead of FFT axes: the FFT twiddle
+    tables that follow an odd-length table must stay 8-byte aligned."""
+    nx, ny, nz = 37, 64, 128
+    mx = 2 * (nx // 2 + 1)
+    rng = np.random.default_rng(5)
+    den = np.zeros((nz, ny, mx), np.float32)
+    den[:, :, :nx] = (rng.random((nz, ny, nx)) ** 6 * 1e3).astype(np.float32)
+    den = den.ravel()
+    _, exact = restatement.smooth(den, nx, ny, nz, 0.005, 0.0075)
+    got = den.copy()
+    dropin.gaussian_Smoothing(got, nx, ny, nz, 0.005, 0.0075)
+    a, b = _logical(got, nx, ny, nz), _logical(exact, nx, ny, nz)
+    assert np.abs(a - b).max() / np.abs(b).max() < 2e-6
