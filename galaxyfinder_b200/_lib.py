@@ -146,6 +146,7 @@ SIGNATURES = {
     "gf_mesh_stage": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP, _VP, _INT]),
     "gf_tsc_deposit": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP]),
     "gf_gaussian_smooth": (_INT, [_VP, _I32, _VP, _VP, _VP]),
+    "gf_gaussian_smooth_noalloc": (_INT, [_VP, _INT, _INT, _INT, _D, _F, _VP]),
     "gf_find_den": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP]),
     "gf_tree_build": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _INT, ctypes.POINTER(TreeInfo)]),
     "gf_tree_export": (_INT, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),

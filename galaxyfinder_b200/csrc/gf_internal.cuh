@@ -145,6 +145,20 @@ int launch_scale(gf_ctx *ctx, float *den, int64_t ncells, double factor);
 int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
                   const gf_mesh_desc *mesh_dev, float *den);
 
+// Single-mesh smoothing plan in one contiguous byte blob (see gf_smooth.cu):
+// [mesh desc | 3 axis tables | per axis: halo list, tile prefix | tables].
+constexpr int kNoAllocMaxAxis = 1024;
+struct SingleMeshPlan {
+    size_t bytes;
+    size_t off_mesh, off_axes, off_tables;
+    size_t off_halos[3], off_starts[3];
+    int64_t ntiles[3];
+    int n[3], pmax[3];
+};
+int smooth_single_build(const gf_mesh_desc &m, unsigned char *blob, size_t cap, SingleMeshPlan *plan);
+int smooth_single_launch(gf_ctx *ctx, float *den, const unsigned char *dev_blob,
+                         const SingleMeshPlan &plan);
+
 inline int64_t mesh_cells(const gf_mesh_desc &m) {
     return (int64_t)(2 * (m.nx / 2 + 1)) * m.ny * m.nz;
 }

@@ -553,3 +553,124 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
 }
 
 }  // namespace gf
+
+// ------------------------------------------------------------------------
+// Single-mesh planning into a caller-provided byte buffer (no heap, no device
+// allocation) and the matching launches; used by the allocation-free entry
+// point in gf_noalloc.cu.
+namespace gf {
+
+namespace {
+
+// Tables of one axis written straight into `out` (same layouts as
+// append_tables); returns the float count or -1 if `cap` is too small.
+int64_t write_axis_tables(int n, double rg_cells, float *out, int64_t cap) {
+    const PathKind pk = path_of(n);
+    int64_t k = 0;
+    if (pk != PATH_DIRECT) {
+        const int ntw = pk == PATH_FFT8 ? n : n / 2;
+        if (cap < 2 * (int64_t)ntw + n) return -1;
+        for (int i = 0; i < ntw; i++) {
+            const double ang = 2.0 * M_PI * (double)i / (double)n;
+            out[k++] = (float)cos(ang);
+            out[k++] = (float)-sin(ang);
+        }
+        for (int i = 0; i < n; i++) out[k++] = (float)(axis_factor(i, n, rg_cells) / n);
+    } else {
+        if (cap < n || n > kNoAllocMaxAxis) return -1;
+        double g[kNoAllocMaxAxis];
+        for (int i = 0; i < n; i++) g[i] = axis_factor(i, n, rg_cells);
+        for (int mm = 0; mm < n; mm++) {
+            double acc = 0.0;
+            for (int i = 0; i < n; i++) acc += g[i] * cos(2.0 * M_PI * (double)(((long)i * mm) % n) / n);
+            out[k++] = (float)(acc / n);
+        }
+    }
+    return k;
+}
+
+}  // namespace
+
+int smooth_single_build(const gf_mesh_desc &m, unsigned char *blob, size_t cap, SingleMeshPlan *plan) {
+    if (m.nx < 1 || m.ny < 1 || m.nz < 1 || !(m.cellsize > 0) || m.nx > kNoAllocMaxAxis ||
+        m.ny > kNoAllocMaxAxis || m.nz > kNoAllocMaxAxis) {
+        set_status(GF_EINVAL, "mesh %d x %d x %d: every axis must be 1..%d for the allocation-free "
+                   "smoothing", m.nx, m.ny, m.nz, kNoAllocMaxAxis);
+        return GF_EINVAL;
+    }
+    auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
+    size_t off = 0;
+    plan->off_mesh = off;
+    off = align(off + sizeof(gf_mesh_desc));
+    plan->off_axes = off;
+    off = align(off + 3 * sizeof(AxisTable));
+    for (int a = 0; a < 3; a++) {
+        plan->off_halos[a] = off;
+        off = align(off + sizeof(int32_t));
+        plan->off_starts[a] = off;
+        off = align(off + 2 * sizeof(int64_t));
+    }
+    plan->off_tables = off;
+    if (off > cap) {
+        set_status(GF_EINVAL, "allocation-free smoothing: scratch too small");
+        return GF_EINVAL;
+    }
+    gf_mesh_desc md = m;
+    md.off = 0;
+    memcpy(blob + plan->off_mesh, &md, sizeof(md));
+    const double rg_cells = (double)(float)(m.rg / m.cellsize);  // gsmooth.c:67
+    const int dims[3] = {m.nx, m.ny, m.nz};
+    AxisTable at[3];
+    float *tab = reinterpret_cast<float *>(blob + plan->off_tables);
+    const int64_t tcap = (int64_t)((cap - plan->off_tables) / sizeof(float));
+    int64_t used = 0;
+    for (int a = 0; a < 3; a++) {
+        const int n = dims[a];
+        at[a].n = n;
+        at[a].logn = path_of(n) == PATH_DIRECT ? -1 : ilog2_exact(n);
+        used = (used + 3) & ~int64_t(3);  // 16-byte aligned tables (float2 twiddles)
+        at[a].tab_off = used;
+        const int64_t k = write_axis_tables(n, rg_cells, tab + used, tcap - used);
+        if (k < 0) {
+            set_status(GF_EINVAL, "allocation-free smoothing: tables exceed the scratch");
+            return GF_EINVAL;
+        }
+        used += k;
+        int pmax = 32;
+        if (path_of(n) != PATH_FFT8) {
+            while (pmax > 2 && (size_t)2 * (pmax / 2) * n * sizeof(float2) > 200 * 1024) pmax -= 2;
+        }
+        const int64_t cx = (m.nx + pmax - 1) / pmax;
+        const int64_t nt = a == 0 ? ((int64_t)m.ny * m.nz + pmax - 1) / pmax
+                                  : cx * (a == 1 ? m.nz : m.ny);
+        const int32_t h0 = 0;
+        const int64_t st[2] = {0, nt};
+        memcpy(blob + plan->off_halos[a], &h0, sizeof(h0));
+        memcpy(blob + plan->off_starts[a], st, sizeof(st));
+        plan->ntiles[a] = nt;
+        plan->n[a] = n;
+        plan->pmax[a] = pmax;
+    }
+    memcpy(blob + plan->off_axes, at, sizeof(at));
+    plan->bytes = plan->off_tables + (size_t)used * sizeof(float);
+    return GF_OK;
+}
+
+int smooth_single_launch(gf_ctx *ctx, float *den, const unsigned char *dev_blob,
+                         const SingleMeshPlan &plan) {
+    const gf_mesh_desc *mesh_dev = reinterpret_cast<const gf_mesh_desc *>(dev_blob + plan.off_mesh);
+    const AxisTable *axes = reinterpret_cast<const AxisTable *>(dev_blob + plan.off_axes);
+    const float *tables = reinterpret_cast<const float *>(dev_blob + plan.off_tables);
+    for (int a = 0; a < 3; a++) {
+        GroupLaunch gl;
+        gl.halos = reinterpret_cast<const int32_t *>(dev_blob + plan.off_halos[a]);
+        gl.tile_start = reinterpret_cast<const int64_t *>(dev_blob + plan.off_starts[a]);
+        gl.ngroup = 1;
+        if (a == 0) GF_TRY(launch_group<0>(ctx, den, mesh_dev, gl, plan.ntiles[a], plan.n[a], plan.pmax[a], axes, tables));
+        else if (a == 1) GF_TRY(launch_group<1>(ctx, den, mesh_dev, gl, plan.ntiles[a], plan.n[a], plan.pmax[a], axes, tables));
+        else GF_TRY(launch_group<2>(ctx, den, mesh_dev, gl, plan.ntiles[a], plan.n[a], plan.pmax[a], axes, tables));
+    }
+    return GF_OK;
+}
+
+}  // namespace gf

@@ -149,6 +149,19 @@ typedef struct gf_mesh_rule {
 int gf_plan_meshes(int32_t nhalo, const double *extent, const gf_mesh_rule *rule,
                    gf_mesh_desc *desc, int64_t *total_cells);
 
+/* Gaussian smoothing of one caller-owned device mesh (mx*ny*nz floats, in
+ * place) on the caller's stream, allocating nothing.  No counterpart in the
+ * reference: it serves callers that cannot allocate device memory (a fixed
+ * budget owned by another allocator, or a path that cannot afford an
+ * allocation's synchronisation).  Its scratch is a 64 KiB static device array
+ * that every GPU loading libgf holds until exit; each axis must be at most
+ * 1024 cells (GF_EINVAL otherwise).  The first call on a device looks up the
+ * array's device address with that device current, so make it before any
+ * stream capture.  All calls share the array: calls that may overlap on the
+ * GPU (different streams without ordering) race and must be serialised. */
+int gf_gaussian_smooth_noalloc(float *den, int nx, int ny, int nz, double cellsize, float RG,
+                               void *stream);
+
 /* Mesh stage on a batch whose meshes are already described: zero + TSC
  * deposit (tsc_omp2.c:166), Gaussian smoothing (gsmooth.c:14) and the
  * interpolation back to every particle (tsc_omp2.c:40).  den must hold the
