@@ -262,9 +262,15 @@ def main():
     total_particles = sum_over_ranks(float(hb.n))
     value = total_particles / (ms / 1e3)
 
-    # ---- per-phase times (one instrumented step, same work)
+    # ---- per-phase times (CUDA events between the phases of one step), then
+    # the work counters from a separately instrumented step
     _, st = batch.stage_run(ctx, db, cfg, out, stats=True)
     phases = {k[3:]: st[k] for k in st if k.startswith("ms_") and k != "ms_pad"}
+    cfg_count = batch.stage_config(mesh=mesh_rule, knn_k=K_NEIGH, count_work=True)
+    _, stc = batch.stage_run(ctx, db, cfg_count, out, stats=True)
+    for key in ("pp_interactions", "pc_interactions", "knn_nodes", "knn_batches",
+                "knn_candidates", "knn_single_inserts", "knn_bitonic_merges"):
+        st[key] = stc[key]
 
     # ---- e2e through the public API with pinned host buffers
     hx = {k: torch.from_numpy(np.ascontiguousarray(getattr(hb, k))).pin_memory()
@@ -342,6 +348,9 @@ def main():
         "phases_ms": phases,
         "interactions": {"particle_particle": st["pp_interactions"],
                          "particle_cell": st["pc_interactions"]},
+        "knn_work_per_query": {k[4:]: st[k] / max(hb.n, 1) for k in
+                               ("knn_nodes", "knn_batches", "knn_candidates",
+                                "knn_single_inserts", "knn_bitonic_merges")},
         "gpu_launches": int(launches),
         "clocks": clk,
     })

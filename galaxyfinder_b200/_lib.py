@@ -76,7 +76,7 @@ class StageConfig(ctypes.Structure):
         ("mesh", MeshRule), ("box", ctypes.c_double), ("knn_k", ctypes.c_int32),
         ("do_mesh", ctypes.c_int32), ("do_potential", ctypes.c_int32), ("ndirect", ctypes.c_int32),
         ("theta2", ctypes.c_float), ("add_bg", ctypes.c_int32), ("q5_asbuilt", ctypes.c_int32),
-        ("reserved", ctypes.c_int32), ("potentfact", ctypes.c_double),
+        ("count_work", ctypes.c_int32), ("potentfact", ctypes.c_double),
     ]
 
 
@@ -96,6 +96,9 @@ class StageStats(ctypes.Structure):
         ("ms_recentre", ctypes.c_float), ("ms_tree", ctypes.c_float), ("ms_knn", ctypes.c_float),
         ("ms_tsc", ctypes.c_float), ("ms_smooth", ctypes.c_float), ("ms_findden", ctypes.c_float),
         ("ms_potential", ctypes.c_float), ("ms_pad", ctypes.c_float),
+        ("knn_nodes", ctypes.c_uint64), ("knn_batches", ctypes.c_uint64),
+        ("knn_candidates", ctypes.c_uint64), ("knn_single_inserts", ctypes.c_uint64),
+        ("knn_bitonic_merges", ctypes.c_uint64),
     ]
 
 
@@ -106,9 +109,9 @@ BH_NODE_DTYPE = np.dtype([
 ])
 KNN_NODE_DTYPE = np.dtype([
     ("lo", "<f4", (3,)), ("hi", "<f4", (3,)), ("skip", "<i4"), ("lstart", "<i4"),
-    ("lcount", "<i4"), ("count", "<i4"),
+    ("lcount", "<i4"), ("count", "<i4"), ("parent", "<i4"), ("pad", "<i4"),
 ])
-assert BH_NODE_DTYPE.itemsize == 80 and KNN_NODE_DTYPE.itemsize == 40
+assert BH_NODE_DTYPE.itemsize == 80 and KNN_NODE_DTYPE.itemsize == 48
 
 
 class GFError(RuntimeError):

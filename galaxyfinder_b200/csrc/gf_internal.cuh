@@ -85,6 +85,8 @@ struct KnnNode {
     int32_t lstart;  // first loose particle (tree order)
     int32_t lcount;
     int32_t count;   // particles in the subtree: [lstart, lstart + count)
+    int32_t parent;  // preorder index of the parent node, -1 for a halo root
+    int32_t pad;
 };
 
 // Node of the potential walk (preorder): monopole + quadrupole about the
@@ -107,6 +109,7 @@ struct TreeView {
     const KnnNode *knn = nullptr;
     const BhNode *bh = nullptr;
     const int32_t *phalo = nullptr; // tree order -> halo
+    const int32_t *owner = nullptr; // tree order -> preorder node holding it as loose
 };
 
 }  // namespace gf

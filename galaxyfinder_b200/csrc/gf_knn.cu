@@ -9,6 +9,10 @@
 //     for the first query of a chunk, of the 32 tree-order neighbours): any k
 //     distinct particles bound the true k-th distance from above, so the walk
 //     prunes from its first node;
+//   * the walk expands bottom-up from the query's own node (its subtree, then
+//     each ancestor's loose particles and other children) and stops once the
+//     ball of the bound lies inside the processed subtree's box, so the list
+//     fills with close particles first and the bound tightens early;
 //   * a node is skipped when the lower bound of its box distance exceeds the
 //     bound; otherwise its loose particles are tested 32 at a time, one per
 //     lane, and the accepted ones are merged into the list (one warp-wide
@@ -99,29 +103,29 @@ __device__ __forceinline__ float f_box_lb2(const float4 &q, const KnnNode &nd) {
 }
 
 // Merges the candidates of one 32-lane batch (lanes with acc set) into the
-// sorted list (Ld, Li, Lt): one insertion per candidate when there are few,
+// sorted list (Ld, Li): one insertion per candidate when there are few,
 // otherwise a bitonic sort of the batch and a bitonic merge with the list.
-__device__ __forceinline__ void merge_batch(unsigned mask, double cd, int ci, int ct, double &Ld,
-                                            int &Li, int &Lt, int &cnt, int kk, double &bd,
-                                            int &bi) {
+__device__ __forceinline__ void merge_batch(unsigned mask, double cd, int ci, double &Ld, int &Li,
+                                            int &cnt, int kk, double &bd, int &bi,
+                                            unsigned long long &nsingle,
+                                            unsigned long long &nbitonic) {
     const int lane = threadIdx.x & 31;
     const int m = __popc(mask);
     if (m <= 3) {
+        nsingle += m;
         while (mask) {
             const int src = __ffs(mask) - 1;
             mask &= mask - 1;
             const double xd = __shfl_sync(0xffffffffu, cd, src);
             const int xi = __shfl_sync(0xffffffffu, ci, src);
-            const int xt = __shfl_sync(0xffffffffu, ct, src);
             if (key_lt(bd, bi, xd, xi)) continue;  // the bound tightened meanwhile
             const int at = __popc(__ballot_sync(0xffffffffu, lane < kk && key_lt(Ld, Li, xd, xi)));
             const double ud = __shfl_up_sync(0xffffffffu, Ld, 1);
             const int ui = __shfl_up_sync(0xffffffffu, Li, 1);
-            const int ut = __shfl_up_sync(0xffffffffu, Lt, 1);
             if (lane == at) {
-                Ld = xd; Li = xi; Lt = xt;
+                Ld = xd; Li = xi;
             } else if (lane > at) {
-                Ld = ud; Li = ui; Lt = ut;
+                Ld = ud; Li = ui;
             }
             if (cnt < kk) cnt++;
             if (cnt == kk) {
@@ -131,37 +135,22 @@ __device__ __forceinline__ void merge_batch(unsigned mask, double cd, int ci, in
         }
         return;
     }
+    nbitonic++;
     double d = (mask >> lane) & 1 ? cd : kInf;
     int i = (mask >> lane) & 1 ? ci : INT_MAX;
-    int t = ct;
-    // bitonic sort of the batch, carrying the tree index
-#pragma unroll
-    for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            const double od = __shfl_xor_sync(0xffffffffu, d, stride);
-            const int oi = __shfl_xor_sync(0xffffffffu, i, stride);
-            const int ot = __shfl_xor_sync(0xffffffffu, t, stride);
-            const bool up = (lane & size) == 0 || size == 32;
-            const bool lower = (lane & stride) == 0;
-            const bool lt = key_lt(d, i, od, oi);
-            if (!((lower == up) ? lt : !lt)) { d = od; i = oi; t = ot; }
-        }
-    }
+    warp_sort(d, i);
     // the 32 smallest of list and batch: elementwise min with the reversed batch
     const double rd = __shfl_sync(0xffffffffu, d, 31 - lane);
     const int ri = __shfl_sync(0xffffffffu, i, 31 - lane);
-    const int rt = __shfl_sync(0xffffffffu, t, 31 - lane);
-    if (key_lt(rd, ri, Ld, Li)) { Ld = rd; Li = ri; Lt = rt; }
+    if (key_lt(rd, ri, Ld, Li)) { Ld = rd; Li = ri; }
     // bitonic clean to ascending order
 #pragma unroll
     for (int stride = 16; stride > 0; stride >>= 1) {
         const double od = __shfl_xor_sync(0xffffffffu, Ld, stride);
         const int oi = __shfl_xor_sync(0xffffffffu, Li, stride);
-        const int ot = __shfl_xor_sync(0xffffffffu, Lt, stride);
         const bool lower = (lane & stride) == 0;
         const bool lt = key_lt(Ld, Li, od, oi);
-        if (!(lower ? lt : !lt)) { Ld = od; Li = oi; Lt = ot; }
+        if (!(lower ? lt : !lt)) { Ld = od; Li = oi; }
     }
     cnt = min(cnt + m, 32);
     if (cnt >= kk) {
@@ -170,13 +159,105 @@ __device__ __forceinline__ void merge_batch(unsigned mask, double cd, int ci, in
     }
 }
 
+struct ListState {
+    double Ld;  // list entry of this lane (distance^2)
+    int Li;     // list entry of this lane (batch index)
+    int cnt;    // entries filled
+    int kk;     // neighbours wanted
+    double bd;  // bound: accept keys <= (bd, bi)
+    int bi;
+};
+
+template <bool COUNT>
+__device__ __forceinline__ void scan_loose(int l0, int l1, const float4 &Q,
+                                           const float4 *__restrict__ pos,
+                                           const int32_t *__restrict__ perm, ListState &L,
+                                           unsigned long long (&ctr)[5]) {
+    const int lane = threadIdx.x & 31;
+    for (int base = l0; base < l1; base += 32) {
+        const int jj = base + lane;
+        double cd = kInf;
+        int ci = INT_MAX;
+        bool acc = false;
+        if (jj < l1) {
+            const float4 S = pos[jj];
+            if (f_d2(Q, S) <= (float)L.bd * (1.f + kSlack)) {
+                cd = exact_d2(Q, S);
+                ci = perm[jj];
+                acc = !key_lt(L.bd, L.bi, cd, ci);  // (cd, ci) <= (bd, bi)
+            }
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, acc);
+        if (COUNT) {
+            ctr[1]++;
+            ctr[2] += __popc(mask);
+        }
+        if (mask) merge_batch(mask, cd, ci, L.Ld, L.Li, L.cnt, L.kk, L.bd, L.bi, ctr[3], ctr[4]);
+    }
+}
+
+// Visits the preorder nodes [i0, i1) with pruning: a node whose box lies
+// beyond the bound skips its subtree, otherwise its loose particles are
+// scanned and the walk continues at its first child.  The nodes are read 32
+// at a time, one per lane, with their box lower bounds; the serial walk then
+// reads a node's bound with one shuffle and compares it with the current
+// (tightening) bound.
+template <bool COUNT>
+__device__ __forceinline__ void walk_range(int i0, int i1, const float4 &Q,
+                                           const float4 *__restrict__ pos,
+                                           const int32_t *__restrict__ perm,
+                                           const KnnNode *__restrict__ nodes, ListState &L,
+                                           unsigned long long (&ctr)[5]) {
+    const int lane = threadIdx.x & 31;
+    int node = i0;
+    while (node < i1) {
+        const int wb = node;
+        const int j = wb + lane;
+        float lb = __int_as_float(0x7f800000);  // +inf: beyond the range
+        int skip = 0, l0 = 0, lc = 0;
+        if (j < i1) {
+            const KnnNode nd = nodes[j];
+            lb = f_box_lb2(Q, nd);
+            skip = nd.skip;
+            l0 = nd.lstart;
+            lc = nd.lcount;
+        }
+        while (node < i1 && node - wb < 32) {
+            const int li = node - wb;
+            if (COUNT) ctr[0]++;
+            const float nlb = __shfl_sync(0xffffffffu, lb, li);
+            if (nlb > (float)L.bd * (1.f + kSlack)) {
+                node = __shfl_sync(0xffffffffu, skip, li);
+                continue;
+            }
+            const int s0 = __shfl_sync(0xffffffffu, l0, li);
+            const int sc = __shfl_sync(0xffffffffu, lc, li);
+            scan_loose<COUNT>(s0, s0 + sc, Q, pos, perm, L, ctr);
+            node = node + 1;
+        }
+    }
+}
+
+// True when the ball of radius sqrt(bd) around q lies inside the node's box
+// (tested in double with a relative and absolute margin).
+__device__ __forceinline__ bool ball_inside(const float4 &Q, double bd, const KnnNode &A) {
+    const double r = sqrt(bd) * (1.0 + 1e-9) + 1e-12;
+    const double qx = Q.x, qy = Q.y, qz = Q.z;
+    return qx - r >= (double)A.lo[0] && qx + r <= (double)A.hi[0] && qy - r >= (double)A.lo[1] &&
+           qy + r <= (double)A.hi[1] && qz - r >= (double)A.lo[2] && qz + r <= (double)A.hi[2];
+}
+
+template <bool COUNT>
 __global__ void __launch_bounds__(256)
 knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__restrict__ perm,
-           const int32_t *__restrict__ phalo, const int64_t *__restrict__ pstart,
-           const int32_t *__restrict__ root, const int32_t *__restrict__ rend,
+           const float4 *__restrict__ pos_batch, const int32_t *__restrict__ phalo,
+           const int64_t *__restrict__ pstart, const int32_t *__restrict__ owner,
            const KnnNode *__restrict__ nodes, int32_t *__restrict__ nearindex,
-           float *__restrict__ dens, int *err) {
+           float *__restrict__ dens, int *err, unsigned long long *__restrict__ counters) {
     const int lane = threadIdx.x & 31;
+    // work counters: nodes tested, 32-wide leaf batches, candidates that pass
+    // the float filter, candidates inserted one by one, bitonic batch merges
+    unsigned long long ctr[5] = {0, 0, 0, 0, 0};
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t ntask = (n + kChunk - 1) / kChunk;
@@ -184,8 +265,9 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
         const int64_t q0 = task * kChunk;
         const int64_t q1 = min(q0 + kChunk, n);
         int prev_h = -1, prev_ok = 0;
-        double Ld = kInf;
-        int Li = INT_MAX, Lt = 0;
+        ListState L;
+        L.Ld = kInf;
+        L.Li = INT_MAX;
         for (int64_t q = q0; q < q1; q++) {
             const int h = phalo[q];
             const int64_t hs = pstart[h], he = pstart[h + 1];
@@ -198,8 +280,8 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
             int id = INT_MAX;
             if (prev_ok && prev_h == h) {
                 if (lane < kk) {
-                    d = exact_d2(Q, pos[Lt]);
-                    id = Li;
+                    d = exact_d2(Q, pos_batch[L.Li]);
+                    id = L.Li;
                 }
             } else {
                 int64_t w0 = q - 16;
@@ -212,64 +294,56 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
                 }
             }
             warp_sort(d, id);
-            double bd = __shfl_sync(0xffffffffu, d, kk - 1);
-            int bi = __shfl_sync(0xffffffffu, id, kk - 1);
-            Ld = kInf;
-            Li = INT_MAX;
-            Lt = 0;
-            int cnt = 0;
-            int node = root[h];
-            const int end = rend[h];
-            while (node < end) {
-                const KnnNode nd = nodes[node];
-                const float bf = (float)bd * (1.f + kSlack);
-                if (f_box_lb2(Q, nd) > bf) {
-                    node = nd.skip;
-                    continue;
-                }
-                const int l1 = nd.lstart + nd.lcount;
-                for (int base = nd.lstart; base < l1; base += 32) {
-                    const int jj = base + lane;
-                    double cd = kInf;
-                    int ci = INT_MAX;
-                    bool acc = false;
-                    if (jj < l1) {
-                        const float4 S = pos[jj];
-                        if (f_d2(Q, S) <= (float)bd * (1.f + kSlack)) {
-                            cd = exact_d2(Q, S);
-                            ci = perm[jj];
-                            acc = !key_lt(bd, bi, cd, ci);  // (cd, ci) <= (bd, bi)
-                        }
-                    }
-                    const unsigned mask = __ballot_sync(0xffffffffu, acc);
-                    if (mask) merge_batch(mask, cd, ci, jj, Ld, Li, Lt, cnt, kk, bd, bi);
-                }
-                node = node + 1;
+            L.bd = __shfl_sync(0xffffffffu, d, kk - 1);
+            L.bi = __shfl_sync(0xffffffffu, id, kk - 1);
+            L.Ld = kInf;
+            L.Li = INT_MAX;
+            L.cnt = 0;
+            L.kk = kk;
+            // ---- bottom-up expanding walk: q's own node's subtree first, then
+            // each ancestor's loose particles and other children, until the
+            // ball of the bound lies inside the box of the processed subtree
+            // (a node's box lies inside its octant region, which holds exactly
+            // the subtree's particles, so nothing outside can enter the list).
+            int c = owner[q];
+            KnnNode C = nodes[c];
+            walk_range<COUNT>(c, C.skip, Q, pos, perm, nodes, L, ctr);
+            while (C.parent >= 0 && !(L.cnt >= kk && ball_inside(Q, L.bd, C))) {
+                const int a = C.parent;
+                const KnnNode A = nodes[a];
+                if (COUNT) ctr[0]++;
+                scan_loose<COUNT>(A.lstart, A.lstart + A.lcount, Q, pos, perm, L, ctr);
+                walk_range<COUNT>(a + 1, c, Q, pos, perm, nodes, L, ctr);
+                walk_range<COUNT>(C.skip, A.skip, Q, pos, perm, nodes, L, ctr);
+                c = a;
+                C = A;
             }
             prev_h = h;
-            prev_ok = cnt >= kk;
-            if (cnt < kk) {
+            prev_ok = L.cnt >= kk;
+            if (L.cnt < kk) {
                 if (lane == 0) atomicOr(err, GF_ERRBIT_KNN);
                 continue;
             }
             // ---- outputs in batch order
             const int qo = perm[q];
-            if (lane < k) nearindex[(int64_t)qo * k + lane] = lane < kk ? (int32_t)(Li - hs) : -1;
+            if (lane < k) nearindex[(int64_t)qo * k + lane] = lane < kk ? (int32_t)(L.Li - hs) : -1;
             // nnost.c:292,415: maxr = sqrtf(maxdist2); W4(sqrtf(d2_j), maxr/2.)
-            const float neardist = sqrtf((float)__shfl_sync(0xffffffffu, Ld, kk - 1));
+            const float neardist = sqrtf((float)__shfl_sync(0xffffffffu, L.Ld, kk - 1));
             const float hh = (float)(neardist / 2.);
-            const float wj = lane < kk ? w4(sqrtf((float)Ld), hh) : 0.f;
+            const float wj = lane < kk ? w4(sqrtf((float)L.Ld), hh) : 0.f;
             float rho = 0.f;
             for (int j = 0; j < kk; j++) rho += __shfl_sync(0xffffffffu, wj, j);
             if (lane == 0 && dens) dens[qo] = rho;
         }
     }
+    if (COUNT && counters && lane == 0)
+        for (int i = 0; i < 5; i++) atomicAdd(counters + i, ctr[i]);
 }
 
 }  // namespace
 
-int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, int k, int32_t *nearindex,
-               float *dens) {
+int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const float4 *pos_batch, int k,
+               int32_t *nearindex, float *dens, unsigned long long *counters) {
     if (k < 1 || k > 32) {
         set_status(GF_EINVAL, "k = %d: the warp kNN supports 1 <= k <= 32", k);
         return GF_EINVAL;
@@ -279,8 +353,14 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, int k, int
     const int64_t warps_needed = (t.n + kChunk - 1) / kChunk;
     int64_t grid = (warps_needed * 32 + block - 1) / block;
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * 8));
-    knn_kernel<<<(int)grid, block, 0, ctx->stream>>>(t.n, k, t.pos, t.perm, t.phalo, pstart, t.root,
-                                                     t.rend, t.knn, nearindex, dens, ctx->d_err);
+    if (counters)
+        knn_kernel<true><<<(int)grid, block, 0, ctx->stream>>>(t.n, k, t.pos, t.perm, pos_batch, t.phalo,
+                                                               pstart, t.owner, t.knn, nearindex, dens,
+                                                               ctx->d_err, counters);
+    else
+        knn_kernel<false><<<(int)grid, block, 0, ctx->stream>>>(t.n, k, t.pos, t.perm, pos_batch, t.phalo,
+                                                                pstart, t.owner, t.knn, nearindex, dens,
+                                                                ctx->d_err, nullptr);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }

@@ -235,7 +235,17 @@ __device__ __forceinline__ void dft(float2 (&a)[R]) {
     }
 }
 
-// One Stockham radix-R pass over NP complex pencils of length N held in
+// Shared-memory layout of the FFT tiles: complex element k of pencil c sits
+// at c*SN + k + k/8 (one padding slot per 8 elements, pencil stride
+// SN = N + N/8 + 1), so the radix-8 strided stores and the 16-pencil
+// column loads of the y/z passes spread over all 32 banks.
+template <int N>
+struct FftLayout {
+    static constexpr int SN = N + N / 8 + 1;
+    __device__ static __forceinline__ int at(int c, int k) { return c * SN + k + (k >> 3); }
+};
+
+// One Stockham radix-R pass over npair complex pencils of length N held in
 // shared memory (src -> dst), stride S = product of the radices already done:
 //   y[q + S (R p + j)] = w^(p S j) * sum_r x[q + S (p + r M)] e^{-+2 pi i r j/R},
 // M = N/(S R), w = e^{-2 pi i/N} (table tw, conjugated for the inverse).  The
@@ -244,6 +254,7 @@ template <int N, int R, int S, bool INV, bool FILTER>
 __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, float2 *__restrict__ dst,
                                               int npair, const float2 *__restrict__ tw,
                                               const float *__restrict__ filt) {
+    using L = FftLayout<N>;
     constexpr int M = N / (S * R);
     constexpr int ITEMS = N / R;  // butterflies per pencil
     for (int e = threadIdx.x; e < npair * ITEMS; e += blockDim.x) {
@@ -251,11 +262,9 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, fl
         const int t = e - c * ITEMS;
         const int q = t % S;
         const int p = t / S;
-        const float2 *x = src + c * N;
-        float2 *y = dst + c * N;
         float2 a[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) a[r] = x[q + S * (p + r * M)];
+        for (int r = 0; r < R; r++) a[r] = src[L::at(c, q + S * (p + r * M))];
         dft<R, INV>(a);
 #pragma unroll
         for (int j = 1; j < R; j++) {
@@ -272,13 +281,13 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, fl
                 v.x *= g;
                 v.y *= g;
             }
-            y[k] = v;
+            dst[L::at(c, k)] = v;
         }
     }
     __syncthreads();
 }
 
-// Forward FFT, filter, inverse FFT of every pencil pair; result in buf[0].
+// Forward FFT, filter, inverse FFT of every pencil pair; result in b0.
 template <int LOGN>
 __device__ __forceinline__ void fft_filter_ifft(float2 *b0, float2 *b1, int npair, const float2 *tw,
                                                 const float *filt) {
@@ -309,6 +318,7 @@ __global__ void __launch_bounds__((kPencils / 2) * (1 << LOGN) / 8)
 smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh, GroupLaunch g,
                   const AxisTable *__restrict__ axes, const float *__restrict__ tables) {
     constexpr int N = 1 << LOGN;
+    using L = FftLayout<N>;
     extern __shared__ float2 smem[];
     const SmoothTile t = decode_group_tile<AXIS>(blockIdx.x, g, mesh, kPencils);
     const gf_mesh_desc m = mesh[t.halo];
@@ -316,16 +326,21 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
     const int64_t mx = 2 * (m.nx / 2 + 1);
     const int npair = (t.npen + 1) >> 1;
     float2 *b0 = smem;
-    float2 *b1 = smem + (kPencils / 2) * N;
+    float2 *b1 = smem + (kPencils / 2) * L::SN;
     float *fa = reinterpret_cast<float *>(b0);
+    // element (pencil p, position s) lives at base + p*pstride + s*sstride
+    int64_t base, pstride, sstride;
+    if (AXIS == 0) { base = m.off + mx * t.base; pstride = mx; sstride = 1; }
+    else if (AXIS == 1) { base = m.off + t.base + mx * (int64_t)m.ny * t.other; pstride = 1; sstride = mx; }
+    else { base = m.off + t.base + mx * (int64_t)t.other; pstride = 1; sstride = mx * (int64_t)m.ny; }
+    const float *gsrc = den + base;
     const int total = 2 * npair * N;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
         int p, s;
         if (AXIS == 0) { p = e >> LOGN; s = e & (N - 1); }
         else { s = e / (2 * npair); p = e - s * (2 * npair); }
-        float v = 0.f;
-        if (p < t.npen) v = den[elem_addr<AXIS>(m, mx, t, p, s)];
-        fa[2 * ((p >> 1) * N + s) + (p & 1)] = v;
+        const float v = p < t.npen ? gsrc[p * pstride + s * sstride] : 0.f;
+        fa[2 * L::at(p >> 1, s) + (p & 1)] = v;
     }
     __syncthreads();
     // full twiddle table e^{-2 pi i k/N}, k < N, then N filter factors G/N
@@ -333,11 +348,12 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
     const float *filt = tables + at.tab_off + 2 * N;
     fft_filter_ifft<LOGN>(b0, b1, npair, tw, filt);
     const float *fs = reinterpret_cast<const float *>(b0);
+    float *gdst = den + base;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
         int p, s;
         if (AXIS == 0) { p = e >> LOGN; s = e & (N - 1); }
         else { s = e / (2 * npair); p = e - s * (2 * npair); }
-        if (p < t.npen) den[elem_addr<AXIS>(m, mx, t, p, s)] = fs[2 * ((p >> 1) * N + s) + (p & 1)];
+        if (p < t.npen) gdst[p * pstride + s * sstride] = fs[2 * L::at(p >> 1, s) + (p & 1)];
     }
 }
 
@@ -404,7 +420,7 @@ int launch_fft(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunc
                const AxisTable *axes, const float *tables) {
     constexpr int N = 1 << LOGN;
     const int threads = (kPencils / 2) * N / 8;
-    const size_t smem = (size_t)2 * (kPencils / 2) * N * sizeof(float2);
+    const size_t smem = (size_t)2 * (kPencils / 2) * FftLayout<N>::SN * sizeof(float2);
     GF_CUDA_TRY(cudaFuncSetAttribute(smooth_fft_kernel<AXIS, LOGN>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     smooth_fft_kernel<AXIS, LOGN><<<(unsigned)ntiles, threads, smem, ctx->stream>>>(den, mesh_dev, g,

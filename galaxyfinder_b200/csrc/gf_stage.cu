@@ -105,7 +105,8 @@ int gf_knn_density(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_
     std::lock_guard<std::mutex> g(ctx->lock);
     GF_TRY(build_tree(ctx, nhalo, n, pstart_dev, reinterpret_cast<const float4 *>(pos4_dev), 0.5f,
                       0, &ctx->last_tree));
-    GF_TRY(launch_knn(ctx, ctx->last_tree, pstart_dev, k, nearindex, dens));
+    GF_TRY(launch_knn(ctx, ctx->last_tree, pstart_dev, reinterpret_cast<const float4 *>(pos4_dev), k,
+                      nearindex, dens));
     return check_device_errors(ctx);
 }
 
@@ -180,7 +181,13 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
             set_status(GF_EINVAL, "knn_k > 0 needs nearindex");
             return GF_EINVAL;
         }
-        GF_TRY(launch_knn(ctx, ctx->last_tree, b->pstart, cfg->knn_k, o->nearindex, o->dens_sph));
+        unsigned long long *kc = nullptr;
+        if (st && cfg->count_work) {
+            GF_TRY(ctx->tmp[4].reserve(128));
+            kc = ctx->tmp[4].as<unsigned long long>() + 4;
+            GF_CUDA_TRY(cudaMemsetAsync(kc, 0, 5 * sizeof(unsigned long long), s));
+        }
+        GF_TRY(launch_knn(ctx, ctx->last_tree, b->pstart, pos, cfg->knn_k, o->nearindex, o->dens_sph, kc));
     }
     tm.mark();  // 3
     // ---- 4. TSC mesh -> smoothing -> findDen
@@ -204,8 +211,8 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
     // ---- 5. potential
     unsigned long long *counters = nullptr;
     if (cfg->do_potential) {
-        if (st) {
-            GF_TRY(ctx->tmp[4].reserve(64));
+        if (st && cfg->count_work) {
+            GF_TRY(ctx->tmp[4].reserve(128));
             counters = ctx->tmp[4].as<unsigned long long>();
             GF_CUDA_TRY(cudaMemsetAsync(counters, 0, 16, s));
         }
@@ -228,11 +235,20 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         st->ms_smooth = tm.ms(4);
         st->ms_findden = tm.ms(5);
         st->ms_potential = tm.ms(6);
-        if (counters) {
-            unsigned long long hcnt[2] = {0, 0};
-            cudaMemcpy(hcnt, counters, 16, cudaMemcpyDeviceToHost);
-            st->pp_interactions = hcnt[0];
-            st->pc_interactions = hcnt[1];
+        if (cfg->count_work && ctx->tmp[4].ptr) {
+            unsigned long long hcnt[9] = {0};
+            cudaMemcpy(hcnt, ctx->tmp[4].ptr, sizeof(hcnt), cudaMemcpyDeviceToHost);
+            if (counters) {
+                st->pp_interactions = hcnt[0];
+                st->pc_interactions = hcnt[1];
+            }
+            if (cfg->knn_k > 0) {
+                st->knn_nodes = hcnt[4];
+                st->knn_batches = hcnt[5];
+                st->knn_candidates = hcnt[6];
+                st->knn_single_inserts = hcnt[7];
+                st->knn_bitonic_merges = hcnt[8];
+            }
         }
     }
     return status;
@@ -280,7 +296,7 @@ int do_findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex,
     pack_pos_kernel<<<grid1(np), 256, 0, ctx->stream>>>(np, dx, dx + n, dx + 2 * n, nullptr, dx + 3 * n, pos);
     GF_LAUNCH_CHECK();
     GF_TRY(build_tree(ctx, 1, np, dpstart, pos, 0.5f, 0, &ctx->last_tree));
-    GF_TRY(launch_knn(ctx, ctx->last_tree, dpstart, numnear, near32, dens));
+    GF_TRY(launch_knn(ctx, ctx->last_tree, dpstart, pos, numnear, near32, dens));
     GF_TRY(ctx->pin[2].reserve(n * (size_t)numnear * sizeof(int32_t) + n * sizeof(float)));
     int32_t *hn = ctx->pin[2].as<int32_t>();
     GF_CUDA_TRY(cudaMemcpyAsync(hn, near32, n * (size_t)numnear * sizeof(int32_t) + n * sizeof(float),

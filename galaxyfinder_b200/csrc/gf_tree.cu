@@ -52,6 +52,7 @@ struct Build {
     int32_t *ochild;                // 8 child ids or -1
     int32_t *first, *nchild, *lstart, *lcount;
     int32_t *sub, *pre;             // subtree size, preorder index
+    int32_t *par;                   // BFS id of the parent, -1 for roots
     int32_t *counter;               // [0] nodes allocated, [1] overflow flag
 };
 
@@ -61,6 +62,7 @@ __global__ void init_roots(int32_t nhalo, const int64_t *__restrict__ pstart, Bu
     b.start[h] = (int32_t)pstart[h];
     b.count[h] = (int32_t)(pstart[h + 1] - pstart[h]);
     b.halo[h] = h;
+    b.par[h] = -1;
 }
 
 __global__ void init_particles(int64_t n, const int64_t *__restrict__ pstart, int32_t nhalo,
@@ -270,6 +272,7 @@ __global__ void split_nodes(int32_t lvl0, int32_t lvl1, int32_t ncap, Build b) {
             b.start[id] = off;
             b.count[id] = cnt[c];
             b.halo[id] = b.halo[node];
+            b.par[id] = node;
             off += cnt[c];
         }
     }
@@ -330,7 +333,7 @@ __global__ void preorder(int32_t lvl0, int32_t lvl1, Build b) {
 }
 
 __global__ void emit_nodes(int32_t nnode, float theta2, Build b, KnnNode *__restrict__ knn,
-                           BhNode *__restrict__ bh) {
+                           BhNode *__restrict__ bh, int32_t *__restrict__ owner) {
     int node = blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= nnode) return;
     const int i = b.pre[node];
@@ -343,6 +346,9 @@ __global__ void emit_nodes(int32_t nnode, float theta2, Build b, KnnNode *__rest
     k.lstart = b.lstart[node];
     k.lcount = b.lcount[node];
     k.count = b.count[node];
+    k.parent = b.par[node] >= 0 ? b.pre[b.par[node]] : -1;
+    k.pad = 0;
+    for (int j = 0; j < k.lcount; j++) owner[k.lstart + j] = i;
     knn[i] = k;
     BhNode h;
     h.com[0] = b.mx[node];
@@ -417,7 +423,7 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         // ---- node buffers (BFS numbering): exactly the carves below
         const size_t nc = (size_t)ncap;
         const size_t nbytes = 3 * al(nc * 4) + 4 * al(nc * 8) + al(nc * 4) + al(nc * 24) +
-                              al(nc * 24) + 3 * al(nc * 32) + 6 * al(nc * 4) + al(64);
+                              al(nc * 24) + 3 * al(nc * 32) + 7 * al(nc * 4) + al(64);
         GF_TRY(ctx->tree[1].reserve(nbytes + 256));
         char *np_ = ctx->tree[1].as<char>();
         Build b;
@@ -443,6 +449,7 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         b.lcount = carve<int32_t>(np_, nc);
         b.sub = carve<int32_t>(np_, nc);
         b.pre = carve<int32_t>(np_, nc);
+        b.par = carve<int32_t>(np_, nc);
         b.counter = carve<int32_t>(np_, 16);
         cudaStream_t s = ctx->stream;
         GF_CUDA_TRY(cudaMemsetAsync(zero_begin, 0, zero_end - zero_begin, s));
@@ -522,7 +529,7 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         const size_t obytes = al((size_t)std::max(nnode, 1) * sizeof(KnnNode)) +
                               al((size_t)std::max(nnode, 1) * sizeof(BhNode)) +
                               2 * al((size_t)std::max(nhalo, 1) * 4) +
-                              al((size_t)std::max<int64_t>(n, 1) * 4);
+                              2 * al((size_t)std::max<int64_t>(n, 1) * 4);
         GF_TRY(ctx->tree[2].reserve(obytes + 256));
         char *op = ctx->tree[2].as<char>();
         KnnNode *knn = carve<KnnNode>(op, std::max(nnode, 1));
@@ -530,8 +537,9 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         int32_t *root = carve<int32_t>(op, std::max(nhalo, 1));
         int32_t *rend = carve<int32_t>(op, std::max(nhalo, 1));
         int32_t *phalo = carve<int32_t>(op, std::max<int64_t>(n, 1));
+        int32_t *owner = carve<int32_t>(op, std::max<int64_t>(n, 1));
         if (nnode > 0) {
-            emit_nodes<<<grid_exact(nnode, 256), 256, 0, s>>>(nnode, theta2, b, knn, bh);
+            emit_nodes<<<grid_exact(nnode, 256), 256, 0, s>>>(nnode, theta2, b, knn, bh, owner);
             GF_LAUNCH_CHECK();
             emit_roots<<<grid_exact(nhalo, 256), 256, 0, s>>>(nhalo, b, root, rend);
             GF_LAUNCH_CHECK();
@@ -548,6 +556,7 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         out->knn = knn;
         out->bh = bh;
         out->phalo = phalo;
+        out->owner = owner;
         return GF_OK;
     }
     set_status(GF_ENOMEM, "octree node capacity exhausted");

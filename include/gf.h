@@ -196,7 +196,7 @@ typedef struct gf_tree_info {
 int gf_tree_build(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
                   const float *pos4_dev, float theta2, int q5_asbuilt, gf_tree_info *info);
 /* Copies the last tree to host memory: preorder potential nodes (80 bytes
- * each), kNN nodes (40 bytes each), tree-ordered float4 positions, the
+ * each), kNN nodes (48 bytes each), tree-ordered float4 positions, the
  * tree-order -> batch-index permutation and each halo's preorder root/end.
  * Any pointer may be NULL. */
 int gf_tree_export(gf_ctx *ctx, void *bh_nodes, void *knn_nodes, float *pos4, int32_t *perm,
@@ -227,7 +227,7 @@ typedef struct gf_stage_config {
     float theta2;          /* opening parameter (0.5 in the reference) */
     int32_t add_bg;        /* add GetBGpotent of each halo's mass */
     int32_t q5_asbuilt;    /* reproduce ost.c:571's y*x in place of y*z */
-    int32_t reserved;
+    int32_t count_work;    /* with stats: also count kNN/potential work (slower) */
     double potentfact;     /* 0: from gf_get_physics() */
 } gf_stage_config;
 
@@ -244,6 +244,9 @@ typedef struct gf_stage_stats {
     int32_t nhalo, reserved;
     uint64_t pp_interactions, pc_interactions;
     float ms_recentre, ms_tree, ms_knn, ms_tsc, ms_smooth, ms_findden, ms_potential, ms_pad;
+    /* kNN work: nodes tested, 32-wide leaf batches, candidates passing the
+     * float filter, candidates inserted one by one, bitonic batch merges */
+    uint64_t knn_nodes, knn_batches, knn_candidates, knn_single_inserts, knn_bitonic_merges;
 } gf_stage_stats;
 
 /* stats may be NULL; when given, per-phase CUDA-event times are filled in. */

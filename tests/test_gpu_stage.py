@@ -30,7 +30,7 @@ def run(cuda_device):
     hb = synth.catalogue(seed=4242, nhalo=24, nmin=40, nmax=40000, straddle_frac=0.3)
     ctx = batch.Context(0)
     db = batch.DeviceBatch.from_halobatch(hb)
-    cfg = batch.stage_config()
+    cfg = batch.stage_config(count_work=True)
     out, stats = batch.stage_run(ctx, db, cfg, stats=True)
     torch.cuda.synchronize()
     t = {}
