@@ -97,10 +97,13 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
                     const int l1 = nd.lstart + nd.lcount;
                     for (int j = nd.lstart; j < l1; j++) {
                         const float4 S = spos[j];
-                        // ost.c:186-191: float offsets from FP64 positions
-                        const float fx = (float)(px - (double)S.x);
-                        const float fy = (float)(py - (double)S.y);
-                        const float fz = (float)(pz - (double)S.z);
+                        // ost.c:186-191: float offsets of the two positions.  For
+                        // float inputs the FP32 difference is the correctly
+                        // rounded exact difference, i.e. the same bits as
+                        // rounding the FP64 difference.
+                        const float fx = P.x - S.x;
+                        const float fy = P.y - S.y;
+                        const float fz = P.z - S.z;
                         const float r2 = fx * fx + fy * fy + fz * fz;
                         if (r2 > 0.f) acc.add(-S.w * rsqrtf(r2));
                     }

@@ -255,16 +255,25 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, fl
                                               int npair, const float2 *__restrict__ tw,
                                               const float *__restrict__ filt) {
     using L = FftLayout<N>;
-    constexpr int M = N / (S * R);
     constexpr int ITEMS = N / R;  // butterflies per pencil
+    // Inputs of a butterfly: k0 + r N/R; N/R is a multiple of 8 for every
+    // radix plan, so in the padded layout they are base + r (N/R)(9/8).
+    constexpr int IN_STRIDE = N / R + N / (8 * R);
+    // Outputs: kb + S j with kb = q + S R p; for S >= 8 the padded stride is
+    // S (9/8); for S == 1 (first pass, R == 8) kb = 8p and the outputs are
+    // the 8 consecutive padded slots 9p .. 9p + 7.
+    constexpr int OUT_STRIDE = S >= 8 ? S + S / 8 : 1;
+    static_assert(S >= 8 || R == 8, "the first pass is radix 8");
     for (int e = threadIdx.x; e < npair * ITEMS; e += blockDim.x) {
         const int c = e / ITEMS;  // ITEMS is a power of two
         const int t = e - c * ITEMS;
         const int q = t % S;
         const int p = t / S;
+        const int k0 = q + S * p;
+        const float2 *x = src + c * L::SN + k0 + (k0 >> 3);
         float2 a[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) a[r] = src[L::at(c, q + S * (p + r * M))];
+        for (int r = 0; r < R; r++) a[r] = x[r * IN_STRIDE];
         dft<R, INV>(a);
 #pragma unroll
         for (int j = 1; j < R; j++) {
@@ -272,16 +281,17 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, fl
             if (INV) w.y = -w.y;
             a[j] = cmul(a[j], w);
         }
+        const int kb = q + S * R * p;
+        float2 *y = dst + c * L::SN + kb + (kb >> 3);
 #pragma unroll
         for (int j = 0; j < R; j++) {
-            const int k = q + S * (R * p + j);
             float2 v = a[j];
             if (FILTER) {
-                const float g = filt[k];
+                const float g = filt[kb + S * j];
                 v.x *= g;
                 v.y *= g;
             }
-            dst[L::at(c, k)] = v;
+            y[j * OUT_STRIDE] = v;
         }
     }
     __syncthreads();
@@ -328,19 +338,29 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
     float2 *b0 = smem;
     float2 *b1 = smem + (kPencils / 2) * L::SN;
     float *fa = reinterpret_cast<float *>(b0);
-    // element (pencil p, position s) lives at base + p*pstride + s*sstride
-    int64_t base, pstride, sstride;
-    if (AXIS == 0) { base = m.off + mx * t.base; pstride = mx; sstride = 1; }
-    else if (AXIS == 1) { base = m.off + t.base + mx * (int64_t)m.ny * t.other; pstride = 1; sstride = mx; }
-    else { base = m.off + t.base + mx * (int64_t)t.other; pstride = 1; sstride = mx * (int64_t)m.ny; }
+    // element (pencil p, position s) lives at base + p*pstride + s*sstride;
+    // within one tile the offsets fit in 32 bits (axes <= 512, mx*ny < 2^21)
+    int64_t base;
+    int pstride, sstride;
+    if (AXIS == 0) { base = m.off + mx * t.base; pstride = (int)mx; sstride = 1; }
+    else if (AXIS == 1) { base = m.off + t.base + mx * (int64_t)m.ny * t.other; pstride = 1; sstride = (int)mx; }
+    else { base = m.off + t.base + mx * (int64_t)t.other; pstride = 1; sstride = (int)(mx * m.ny); }
     const float *gsrc = den + base;
-    const int total = 2 * npair * N;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        int p, s;
-        if (AXIS == 0) { p = e >> LOGN; s = e & (N - 1); }
-        else { s = e / (2 * npair); p = e - s * (2 * npair); }
-        const float v = p < t.npen ? gsrc[p * pstride + s * sstride] : 0.f;
-        fa[2 * L::at(p >> 1, s) + (p & 1)] = v;
+    const int npen2 = 2 * npair;  // pencils held, the last one zero when npen is odd
+    if (AXIS == 0) {  // rows: consecutive threads walk along a row
+        for (int e = threadIdx.x; e < npen2 * N; e += blockDim.x) {
+            const int p = e >> LOGN, s = e & (N - 1);
+            const float v = p < t.npen ? gsrc[p * pstride + s] : 0.f;
+            fa[2 * L::at(p >> 1, s) + (p & 1)] = v;
+        }
+    } else {  // columns: lane = pencil (consecutive x), warps step along the axis
+        const int p = threadIdx.x & 31;
+        if (p < npen2) {
+            for (int s = threadIdx.x >> 5; s < N; s += blockDim.x >> 5) {
+                const float v = p < t.npen ? gsrc[p + s * sstride] : 0.f;
+                fa[2 * L::at(p >> 1, s) + (p & 1)] = v;
+            }
+        }
     }
     __syncthreads();
     // full twiddle table e^{-2 pi i k/N}, k < N, then N filter factors G/N
@@ -349,11 +369,17 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
     fft_filter_ifft<LOGN>(b0, b1, npair, tw, filt);
     const float *fs = reinterpret_cast<const float *>(b0);
     float *gdst = den + base;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        int p, s;
-        if (AXIS == 0) { p = e >> LOGN; s = e & (N - 1); }
-        else { s = e / (2 * npair); p = e - s * (2 * npair); }
-        if (p < t.npen) gdst[p * pstride + s * sstride] = fs[2 * L::at(p >> 1, s) + (p & 1)];
+    if (AXIS == 0) {
+        for (int e = threadIdx.x; e < npen2 * N; e += blockDim.x) {
+            const int p = e >> LOGN, s = e & (N - 1);
+            if (p < t.npen) gdst[p * pstride + s] = fs[2 * L::at(p >> 1, s) + (p & 1)];
+        }
+    } else {
+        const int p = threadIdx.x & 31;
+        if (p < t.npen) {
+            for (int s = threadIdx.x >> 5; s < N; s += blockDim.x >> 5)
+                gdst[p + s * sstride] = fs[2 * L::at(p >> 1, s) + (p & 1)];
+        }
     }
 }
 
