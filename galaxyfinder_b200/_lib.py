@@ -19,6 +19,7 @@ GF_OK, GF_EINVAL, GF_ENOMEM, GF_EDEVICE, GF_ETIMEOUT, GF_ERANGE, GF_ENOTIMPL = r
 
 # particle types (NewGalFinder/tree.h:47-48)
 TYPE_STAR, TYPE_DM, TYPE_GAS, TYPE_SINK, TYPE_ALL = 1, 2, 3, 4, 5
+GF_UNBOUND, GF_BOUND = 0, 1  # subhaloden.mod6.c:32-33
 
 # SimpleBasicParticleType, NewGalFinder/tree.h:155-162 (88 bytes)
 BP_DTYPE = np.dtype([
@@ -30,6 +31,22 @@ assert BP_DTYPE.itemsize == 88
 
 # Vector3d, NewGalFinder/subhaloden.mod6.c:70-72
 VEC3_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8")])
+
+# Kptype, NewGalFinder/subhaloden.mod6.c:73-77 (48 bytes)
+KP_DTYPE = np.dtype([
+    ("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4"),
+    ("mass", "<f4"), ("bp", "<u8"),
+])
+assert KP_DTYPE.itemsize == 48
+
+# Coretype, NewGalFinder/tree.h:204-213 (56 bytes)
+CORE_DTYPE = np.dtype([
+    ("peak", "<i4"), ("nummem", "<i4"), ("numstar", "<i4"), ("starmass", "<f4"),
+    ("coredensity", "<f4"), ("cx", "<f4"), ("cy", "<f4"), ("cz", "<f4"), ("cvx", "<f4"),
+    ("cvy", "<f4"), ("cvz", "<f4"), ("Rtidal", "<f4"), ("density", "<f4"), ("flag", "u1"),
+    ("_pad", "u1", (3,)),
+])
+assert CORE_DTYPE.itemsize == 56
 
 # gf_mesh_desc (gf.h), 64 bytes
 MESH_DTYPE = np.dtype([
@@ -142,6 +159,10 @@ SIGNATURES = {
     "Self_Halo_Potent": (None, [_INT, _VP, _VP, _VP]),
     "External_Halo_Potent": (None, [_INT, _VP, _VP, _VP, _INT, _VP, _VP]),
     "i_potent_spline": (None, []),
+    "CheckSelfTE": (_INT, [_VP, _INT, _VP, _VP]),
+    "CheckExternalTE": (_INT, [_VP, _INT, _VP, _VP, _INT, _VP]),
+    "gf_tidal_radius": (_INT, [_VP, _INT, _VP, _INT, _VP, _VP, _INT]),
+    "gf_tidal_select": (_INT, [_VP, _INT, _VP, _INT, _F, _F, _F, _F, _VP, ctypes.POINTER(_INT)]),
     "gf_ctx_create": (_INT, [ctypes.POINTER(_VP), _INT, _VP]),
     "gf_ctx_destroy": (_INT, [_VP]),
     "gf_ctx_set_stream": (_INT, [_VP, _VP]),

@@ -5,8 +5,8 @@
 
 Each translation unit under csrc/ is compiled by nvcc for
 ``arch=compute_100a,code=sm_100a`` with ``-lineinfo``; the objects are
-linked into ``galaxyfinder_b200/libgf.so``.  ``gf_tsc.cu`` and ``gf_knn.cu``
-are compiled with ``--fmad=false`` because their results must reproduce the
+linked into ``galaxyfinder_b200/libgf.so``.  ``gf_tsc.cu``, ``gf_knn.cu`` and
+``gf_bound.cu`` are compiled with ``--fmad=false`` because their results must reproduce the
 reference's separately rounded float/double arithmetic bit for bit.
 """
 from __future__ import annotations
@@ -23,7 +23,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libgf.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NOFMAD = {"gf_tsc.cu", "gf_knn.cu"}
+NOFMAD = {"gf_tsc.cu", "gf_knn.cu", "gf_bound.cu"}
 
 
 def nvcc() -> str:

@@ -197,19 +197,53 @@ const gf_physics &physics() {
     return g_phys;
 }
 
-// NFW background potential, subhaloden.mod6.c:1059-1101 (z from amax/a,
-// Comerford concentration, Bryan-Norman style Delta_vir in vv).
-double bg_potent(double mvir) {
+// NFW helpers of subhaloden.mod6.c:1059-1092 with the reference's operand
+// types: amax, a and omep are float, the constants with an L suffix (RHOC,
+// G, 1.L, ...) make their expressions long double (x87 extended precision on
+// x86-64), the C library's double pow/log receive those values rounded to
+// double, and every result is stored as double.  The casts below spell out
+// exactly those conversions (C++ would otherwise pick the long double
+// overloads of pow/log).
+namespace {
+constexpr long double kRhoc = 2.7755E11L;  // RHOC, subhaloden.mod6.c:1081
+constexpr long double kG = 6.672E-8L;      // G, header.h:1
+
+long double nfw_vv() {  // vv, subhaloden.mod6.c:1082
+    const long double om1 = (long double)physics().omep - 1.0L;
+    return 18.0L * (long double)M_PI * (long double)M_PI + 82.0L * om1 -
+           39.0L * (long double)pow((double)om1, 2.0);
+}
+}  // namespace
+
+double nfw_concentration(double mass) {  // get_concentration, :1059-1066
     const gf_physics &ph = physics();
-    const double Msun = 1.989E33, G = 6.672E-8, RHOC = 2.7755E11;
-    double redshift = ph.amax / ph.a - 1.0;
-    double c = 14.5 * pow(mvir / 1.3E13, -0.15) / (1.0 + redshift);
-    double gc = 1. / (log(1.0 + c) - c / (1.0 + c));
-    double omep = ph.omep;
-    double vv = 18.0 * M_PI * M_PI + 82.0 * (omep - 1.0) - 39.0 * pow(omep - 1.0, 2.0);
-    double rvir = pow(3. * mvir / (4.0 * M_PI * vv * RHOC), 0.3333333333333);
-    double vc2 = G * mvir / rvir * ph.potentfact;
-    (void)Msun;
+    const double mstar = (double)1.3E13L;
+    const double redshift = (double)((long double)(ph.amax / ph.a) - 1.0L);
+    return (double)((long double)(14.5 * pow(mass / mstar, -0.15)) / (1.0L + redshift));
+}
+
+double nfw_alpha(double c, double s) {  // get_alpha, :1067-1074
+    const double cs = c * s;
+    const long double t = cs / (1.0L + cs);
+    const double res = (double)(2.0L - t * t);
+    return (double)(res / ((long double)log((double)(1.0L + cs)) - cs / (1.0L + cs)));
+}
+
+double nfw_gnfw(double c) {  // gnfw, :1083-1087
+    return (double)(1. / ((long double)log((double)(1.0L + c)) - c / (1.0L + c)));
+}
+
+double nfw_rvir(double mvir) {  // GetRvir, :1088-1092
+    return pow((double)(3. * mvir / (4.0L * (long double)M_PI * nfw_vv() * kRhoc)),
+               (double)0.3333333333333L);
+}
+
+// GetBGpotent, subhaloden.mod6.c:1093-1101.
+double bg_potent(double mvir) {
+    const double c = nfw_concentration(mvir);
+    const double gc = nfw_gnfw(c);
+    const double rvir = nfw_rvir(mvir);
+    const double vc2 = (double)(kG * mvir / rvir) * physics().potentfact;  // Get_Vc2, :1075-1079
     return vc2 * (1 - gc * log(1 + c));
 }
 

@@ -307,11 +307,15 @@ int do_findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex,
     return GF_OK;
 }
 
-int potent_common(int nend, Vector3d *r, float *penergy, int snp, Vector3d *sr, float *smass,
-                  bool self) {
-    gf_ctx *ctx = default_ctx();
-    if (!ctx) return last_status() ? last_status() : GF_EDEVICE;
-    std::lock_guard<std::mutex> g(ctx->lock);
+}  // namespace
+
+namespace gf {
+
+// Potential of the sources (sr, smass) at the targets r (self: r == sr) on
+// the device of ctx; leaves penergy in device memory (*dout) and the FP64
+// target positions (Vector3d AoS) at *dtargets.  Caller holds ctx->lock.
+int potent_device(gf_ctx *ctx, int nend, const Vector3d *r, int snp, const Vector3d *sr,
+                  const float *smass, bool self, float **dout_ret, const double **dtargets) {
     const size_t ns = (size_t)snp, nt = (size_t)nend;
     // pinned staging: sources (3 doubles + mass), targets (3 doubles), pstart, target count
     const size_t hbytes = ns * 3 * sizeof(double) + ns * sizeof(float) + (self ? 0 : nt * 3 * sizeof(double)) +
@@ -373,7 +377,25 @@ int potent_common(int nend, Vector3d *r, float *penergy, int snp, Vector3d *sr, 
         GF_TRY(launch_external_potential(ctx, ctx->last_tree, dps, nend, tpos, thalo, ntarget_dev,
                                          pp, dout, nullptr));
     }
-    GF_CUDA_TRY(cudaMemcpyAsync(penergy, dout, nt * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    *dout_ret = dout;
+    if (dtargets)
+        *dtargets = reinterpret_cast<const double *>(d + (self ? off_sr : off_tr));
+    return GF_OK;
+}
+
+}  // namespace gf
+
+namespace {
+
+int potent_common(int nend, Vector3d *r, float *penergy, int snp, Vector3d *sr, float *smass,
+                  bool self) {
+    gf_ctx *ctx = default_ctx();
+    if (!ctx) return last_status() ? last_status() : GF_EDEVICE;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    float *dout = nullptr;
+    GF_TRY(potent_device(ctx, nend, r, snp, sr, smass, self, &dout, nullptr));
+    GF_CUDA_TRY(cudaMemcpyAsync(penergy, dout, (size_t)nend * sizeof(float), cudaMemcpyDeviceToHost,
+                                ctx->stream));
     return check_device_errors(ctx);  // synchronises
 }
 

@@ -34,6 +34,21 @@ int launch_external_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pst
                               const int32_t *ntarget_halo, const PotentialParams &pp,
                               float *penergy, float *raw);
 const gf_physics &physics();
+double bg_potent(double mvir);
+// Host NFW helpers (get_concentration, get_alpha, gnfw, GetRvir of
+// subhaloden.mod6.c:1059-1092) in the reference's float/double/long double mix.
+double nfw_concentration(double mass);
+double nfw_alpha(double c, double s);
+double nfw_gnfw(double c);
+double nfw_rvir(double mvir);
+
+// Tree (or direct) potential of the sources (sr, smass) at targets r (self:
+// r == sr) on ctx's device, as Self_Halo_Potent / External_Halo_Potent:
+// penergy = phi * potentfact + GetBGpotent(source mass), left in device memory
+// at *dout; *dtargets (optional) receives the device copy of the FP64 target
+// positions (Vector3d AoS).  The caller holds ctx->lock.
+int potent_device(gf_ctx *ctx, int nend, const Vector3d *r, int snp, const Vector3d *sr,
+                  const float *smass, bool self, float **dout, const double **dtargets);
 
 // Copies the preorder node arrays and particle order to the host (tests).
 int export_tree(gf_ctx *ctx, const TreeView &t, void *knn_host, void *bh_host, float4 *pos_host,

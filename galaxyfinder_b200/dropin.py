@@ -94,6 +94,59 @@ def External_Halo_Potent(r, mass, sr, smass):
     return pe
 
 
+def make_kp(x, y, z, vx, vy, vz, mass, bp=None) -> np.ndarray:
+    """Kptype array (subhaloden.mod6.c:73-77); bp is the SimpleBasicParticleType
+    array whose entries the members point to (for their types)."""
+    kp = np.zeros(len(x), _lib.KP_DTYPE)
+    kp["x"], kp["y"], kp["z"] = x, y, z
+    kp["vx"], kp["vy"], kp["vz"] = vx, vy, vz
+    kp["mass"] = mass
+    if bp is not None:
+        kp["bp"] = bp.ctypes.data + np.arange(len(x), dtype=np.uint64) * np.uint64(_lib.BP_DTYPE.itemsize)
+    return kp
+
+
+def CheckSelfTE(kp, bp_owner=None):
+    """subhaloden.mod6.c:1730 — returns (bound flags, number bound).  bp_owner
+    keeps alive the particle array the kp entries point to."""
+    kp = np.ascontiguousarray(kp)
+    flags = np.zeros(len(kp), np.uint8)
+    nb = lib().CheckSelfTE(ptr(kp), len(kp), ptr(flags), None)
+    check_last()
+    return flags, nb
+
+
+def CheckExternalTE(tkp, skp, core):
+    """subhaloden.mod6.c:1622 — core: one CORE_DTYPE record (centre, velocity)."""
+    tkp, skp = np.ascontiguousarray(tkp), np.ascontiguousarray(skp)
+    core = np.ascontiguousarray(core, _lib.CORE_DTYPE).reshape(-1)
+    flags = np.zeros(len(tkp), np.uint8)
+    nb = lib().CheckExternalTE(ptr(tkp), len(tkp), ptr(flags), ptr(skp), len(skp), ptr(core))
+    check_last()
+    return flags, nb
+
+
+def tidal_radius(core, score_core, bp, haloid):
+    """AdGetTidalRCenterCore (subhaloden.mod6.c:1910): fills core['Rtidal'] and
+    core['nummem'] in place."""
+    score_core = np.ascontiguousarray(score_core, np.int32)
+    haloid = np.ascontiguousarray(haloid, np.int32)
+    _lib.check(lib().gf_tidal_radius(ptr(core), len(core), ptr(score_core), len(score_core),
+                                     ptr(bp), ptr(haloid), len(bp)))
+    return core
+
+
+def tidal_select(bp, cx, cy, cz, rtidal, plist=None):
+    """Tidal cut (subhaloden.mod6.c:2734-2745): indices within rtidal, in order."""
+    n = len(bp) if plist is None else len(plist)
+    pl = None if plist is None else np.ascontiguousarray(plist, np.int32)
+    out = np.zeros(max(n, 1), np.int32)
+    cnt = _lib.ctypes.c_int(0)
+    _lib.check(lib().gf_tidal_select(ptr(bp), len(bp), ptr(pl), n, cx, cy, cz, rtidal, ptr(out),
+                                     _lib.ctypes.byref(cnt)))
+    return out[:cnt.value]
+
+
 def i_potent_spline():
     """force_spline.mod3.c:81 — no table is needed by the GPU kernel."""
     lib().i_potent_spline()

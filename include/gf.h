@@ -86,10 +86,34 @@ void Self_Halo_Potent(int np, Vector3d *r, float *mass, float *penergy);
 /* NewGalFinder/subhaloden.mod6.c:1537 */
 void External_Halo_Potent(int nend, Vector3d *r, float *mass, float *penergy, int snp,
                           Vector3d *sr, float *smass);
+/* NewGalFinder/subhaloden.mod6.c:1730.  Bound flags (GF_BOUND/GF_UNBOUND) of
+ * the members kp[np]: kinetic energy about the stars' centre of mass against
+ * the self potential (Self_Halo_Potent).  Returns the number bound. */
+int CheckSelfTE(Kptype *kp, int np, unsigned char *bndflag, Coretype *icore);
+/* NewGalFinder/subhaloden.mod6.c:1622.  Bound flags of the targets tkp[tnp]
+ * against the potential of the sources skp[snp] (External_Halo_Potent), kinetic
+ * energy about the core's centre and velocity.  Returns the number bound. */
+int CheckExternalTE(Kptype *tkp, int tnp, unsigned char *bndflag, Kptype *skp, int snp,
+                    Coretype *icore);
 /* NewGalFinder/force_spline.mod3.c:81.  The GPU potential evaluates the
  * kernel -1/r and its quadrupole terms exactly, so no table is built; the
  * call only initialises the device. */
 void i_potent_spline(void);
+
+/* Tidal radius of every core: AdGetTidalRCenterCore (subhaloden.mod6.c:1910-2035)
+ * with get_tidal_ellipse (:1102-1165).  The reference reads each particle's
+ * core from its file-global working array (wp[i].haloid); here it is passed
+ * as haloid[np] (negative: no core), and score_core[ncore] lists the core ids
+ * in the reference's score order (increasing member count).  Fills
+ * core[].Rtidal and core[].nummem.  Host pointers, synchronous. */
+int gf_tidal_radius(Coretype *core, int numcore, const int32_t *score_core, int ncore,
+                    const SimpleBasicParticleType *bp, const int32_t *haloid, int np);
+/* Tidal cut of GetMemberRestParticleList (subhaloden.mod6.c:2734-2745) and
+ * GetShellParticleFromRestParticleLIST (:532-541): the entries of plist[nlist]
+ * (all np particles if plist is NULL) whose float distance^2 from (cx, cy, cz)
+ * is below rtidal^2, in list order, into out[]; *nout receives the count. */
+int gf_tidal_select(const SimpleBasicParticleType *bp, int np, const int32_t *plist, int nlist,
+                    float cx, float cy, float cz, float rtidal, int32_t *out, int *nout);
 
 /* ------------------------------------------------------------------------
  * Native batched API.

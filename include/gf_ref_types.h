@@ -6,6 +6,8 @@
  *   SimpleBasicParticleType  NewGalFinder/tree.h:155-162   88 bytes
  *   Vector3d                 NewGalFinder/subhaloden.mod6.c:70-72   24 bytes
  *   Coretype                 NewGalFinder/tree.h:204-213   56 bytes
+ *   Kptype                   NewGalFinder/subhaloden.mod6.c:73-77   48 bytes
+ *   Coresorttype             NewGalFinder/subhaloden.mod6.c:298-301 16 bytes
  *
  * Only the layout is shared; no reference code is included. */
 #ifndef GF_REF_TYPES_H
@@ -44,6 +46,21 @@ typedef struct Coretype {
     float Rtidal, density;
     unsigned char flag;
 } Coretype;
+
+typedef struct Kptype {
+    double x, y, z;
+    float vx, vy, vz, mass;
+    SimpleBasicParticleType *bp;
+} Kptype;
+
+typedef struct Coresorttype {
+    int nmem;
+    Coretype *core;
+} Coresorttype;
+
+/* Bound flags of CheckSelfTE/CheckExternalTE (subhaloden.mod6.c:32-33) */
+#define GF_BOUND 1
+#define GF_UNBOUND 0
 
 #ifdef __cplusplus
 }

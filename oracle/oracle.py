@@ -166,6 +166,11 @@ class Reference:
             L.ref_External_Halo_Potent.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP, _VP, _VP,
                                                    _VP]
             L.ref_tree_potential.argtypes = [_I, _VP, _VP, _VP, _VP, _F, _VP]
+            L.ref_CheckSelfTE.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]
+            L.ref_CheckExternalTE.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP, _VP,
+                                              _VP, _VP, _VP, _VP]
+            L.ref_AdGetTidalRCenterCore.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP, _I, _VP,
+                                                    _VP, _VP]
             if L.ref_init(arena_mb) != 0:
                 raise RuntimeError("reference arena allocation failed")
             Reference._libs[variant] = L
@@ -258,6 +263,43 @@ class Reference:
         self.L.ref_External_Halo_Potent(len(tx), _p(tx), _p(ty), _p(tz), _p(tm), _p(pe), len(sx),
                                         _p(sx), _p(sy), _p(sz), _p(sm))
         return pe
+
+    @staticmethod
+    def _f(a):
+        return np.ascontiguousarray(a, np.float32)
+
+    def CheckSelfTE(self, x, y, z, vx, vy, vz, mass, type_):
+        """subhaloden.mod6.c:1730 -> (bound flags, number bound)."""
+        x, y, z = map(self._d, (x, y, z))
+        vx, vy, vz, m = map(self._f, (vx, vy, vz, mass))
+        t = np.ascontiguousarray(type_, np.int32)
+        flag = np.zeros(len(x), np.uint8)
+        nb = self.L.ref_CheckSelfTE(len(x), _p(x), _p(y), _p(z), _p(vx), _p(vy), _p(vz), _p(m),
+                                    _p(t), _p(flag))
+        return flag, nb
+
+    def CheckExternalTE(self, x, y, z, vx, vy, vz, mass, sx, sy, sz, smass, core6):
+        """subhaloden.mod6.c:1622; core6 = (cx, cy, cz, cvx, cvy, cvz)."""
+        x, y, z, sx, sy, sz = map(self._d, (x, y, z, sx, sy, sz))
+        vx, vy, vz, m, sm, c6 = map(self._f, (vx, vy, vz, mass, smass, core6))
+        flag = np.zeros(len(x), np.uint8)
+        nb = self.L.ref_CheckExternalTE(len(x), _p(x), _p(y), _p(z), _p(vx), _p(vy), _p(vz), _p(m),
+                                        len(sx), _p(sx), _p(sy), _p(sz), _p(sm), _p(c6), _p(flag))
+        return flag, nb
+
+    def AdGetTidalRCenterCore(self, x, y, z, mass, haloid, core6, score_core):
+        """subhaloden.mod6.c:1910 -> (Rtidal, nummem) per core; core6 is
+        (numcore, 6) centres and velocities, score_core the ranked core ids."""
+        x, y, z, mass = map(self._d, (x, y, z, mass))
+        hid = np.ascontiguousarray(haloid, np.int32)
+        c6 = np.ascontiguousarray(core6, np.float32).reshape(-1, 6)
+        sc = np.ascontiguousarray(score_core, np.int32)
+        nc = len(c6)
+        rt = np.zeros(nc, np.float32)
+        nm = np.zeros(nc, np.int32)
+        self.L.ref_AdGetTidalRCenterCore(len(x), _p(x), _p(y), _p(z), _p(mass), _p(hid), nc,
+                                         _p(c6), len(sc), _p(sc), _p(rt), _p(nm))
+        return rt, nm
 
 
 def ref_available() -> bool:

@@ -242,3 +242,88 @@ int ref_tree_potential(int np, const double *x, const double *y, const double *z
     Free(tree);
     return 0;
 }
+
+/* ---- boundedness test and tidal radius (subhaloden.mod6.c) ---- */
+typedef struct Kptype_h {
+    double x, y, z;
+    float vx, vy, vz, mass;
+    SimpleBasicParticleType *bp;
+} Kptype_h;                                                      /* subhaloden.mod6.c:73-77 */
+typedef struct Coresorttype_h { int nmem; Coretype *core; } Coresorttype_h; /* :298-301 */
+typedef struct WorkingParticle_h {
+    float den;
+    int haloid;
+    unsigned char flag;
+    unsigned char flag2[64];
+} WorkingParticle_h;                                             /* :246-251, MAXTHREADS 64 */
+extern WorkingParticle_h *wp;
+int CheckSelfTE(Kptype_h *, int, unsigned char *, Coretype *);
+int CheckExternalTE(Kptype_h *, int, unsigned char *, Kptype_h *, int, Coretype *);
+void AdGetTidalRCenterCore(Coretype *, int, Coresorttype_h *, int, SimpleBasicParticleType *, int);
+
+static Kptype_h *make_kp(int n, const double *x, const double *y, const double *z, const float *vx,
+                         const float *vy, const float *vz, const float *mass,
+                         SimpleBasicParticleType *bp) {
+    Kptype_h *kp = (Kptype_h *)malloc(sizeof(Kptype_h) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; i++) {
+        kp[i].x = x[i]; kp[i].y = y[i]; kp[i].z = z[i];
+        kp[i].vx = vx[i]; kp[i].vy = vy[i]; kp[i].vz = vz[i];
+        kp[i].mass = mass[i];
+        kp[i].bp = bp ? bp + i : NULL;
+    }
+    return kp;
+}
+
+int ref_CheckSelfTE(int np, const double *x, const double *y, const double *z, const float *vx,
+                    const float *vy, const float *vz, const float *mass, const int *type,
+                    unsigned char *flag) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, type, x, y, z, NULL);
+    Kptype_h *kp = make_kp(np, x, y, z, vx, vy, vz, mass, bp);
+    int nb = CheckSelfTE(kp, np, flag, NULL);
+    free(kp);
+    Free(bp);
+    return nb;
+}
+
+int ref_CheckExternalTE(int tnp, const double *x, const double *y, const double *z,
+                        const float *vx, const float *vy, const float *vz, const float *mass,
+                        int snp, const double *sx, const double *sy, const double *sz,
+                        const float *smass, const float *core6, unsigned char *flag) {
+    if (!g_ready) return -1;
+    Kptype_h *tkp = make_kp(tnp, x, y, z, vx, vy, vz, mass, NULL);
+    float *zero = (float *)calloc((size_t)(snp > 0 ? snp : 1), sizeof(float));
+    Kptype_h *skp = make_kp(snp, sx, sy, sz, zero, zero, zero, smass, NULL);
+    Coretype core;
+    memset(&core, 0, sizeof(core));
+    core.cx = core6[0]; core.cy = core6[1]; core.cz = core6[2];
+    core.cvx = core6[3]; core.cvy = core6[4]; core.cvz = core6[5];
+    int nb = CheckExternalTE(tkp, tnp, flag, skp, snp, &core);
+    free(skp); free(zero); free(tkp);
+    return nb;
+}
+
+int ref_AdGetTidalRCenterCore(int np, const double *x, const double *y, const double *z,
+                              const double *mass, const int *haloid, int numcore,
+                              const float *core6, int ncore, const int *score_core,
+                              float *rtidal, int *nummem) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, NULL, x, y, z, mass);
+    WorkingParticle_h *w = (WorkingParticle_h *)calloc((size_t)(np > 0 ? np : 1), sizeof(WorkingParticle_h));
+    for (int i = 0; i < np; i++) w[i].haloid = haloid[i];
+    WorkingParticle_h *saved = wp;
+    wp = w;
+    Coretype *core = (Coretype *)calloc((size_t)numcore, sizeof(Coretype));
+    for (int c = 0; c < numcore; c++) {
+        core[c].cx = core6[6 * c]; core[c].cy = core6[6 * c + 1]; core[c].cz = core6[6 * c + 2];
+        core[c].cvx = core6[6 * c + 3]; core[c].cvy = core6[6 * c + 4]; core[c].cvz = core6[6 * c + 5];
+    }
+    Coresorttype_h *score = (Coresorttype_h *)calloc((size_t)(ncore > 0 ? ncore : 1), sizeof(Coresorttype_h));
+    for (int a = 0; a < ncore; a++) { score[a].core = core + score_core[a]; score[a].nmem = 0; }
+    AdGetTidalRCenterCore(core, numcore, score, ncore, bp, np);
+    for (int c = 0; c < numcore; c++) { rtidal[c] = core[c].Rtidal; nummem[c] = core[c].nummem; }
+    wp = saved;
+    free(score); free(core); free(w);
+    Free(bp);
+    return 0;
+}

@@ -111,8 +111,82 @@ def main():
                         self_small=self_small, ext_pe=ext_pe, potentfact=potentfact,
                         r1kineticfact=r1k, r2kineticfact=r2k,
                         bg_1e12=ref.bg_potent(1e12), bg_mass=ref.bg_potent(float(np.sum(mf, dtype=np.float64))))
+    bound_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
+
+
+def clumps(rng, sizes, centres, sigmas):
+    """Gaussian clumps (one per core) in shuffled particle order, plus 400
+    unassigned background particles (haloid -1)."""
+    pos, hid = [], []
+    for c, (n, ctr, sg) in enumerate(zip(sizes, centres, sigmas)):
+        pos.append(np.asarray(ctr) + sg * rng.standard_normal((n, 3)))
+        hid.append(np.full(n, c, np.int32))
+    pos.append(0.25 + 0.2 * rng.standard_normal((400, 3)))
+    hid.append(np.full(400, -1, np.int32))
+    pos, hid = np.concatenate(pos), np.concatenate(hid)
+    perm = rng.permutation(len(pos))
+    return pos[perm], hid[perm]
+
+
+def bound_fixture(ref):
+    """CheckSelfTE / CheckExternalTE (subhaloden.mod6.c:1730, 1622), the
+    tidal radius (AdGetTidalRCenterCore, :1910) and GetBGpotent (:1093)."""
+    potentfact, r1k, r2k = ref.physics()
+    rng = np.random.default_rng(41)
+    r = blob(41, 3000, 0.03)
+    mf = (10 ** rng.uniform(7, 8.5, len(r))).astype(np.float32)
+    typ = np.where(rng.random(len(r)) < 0.3, 1, 2).astype(np.int32)
+    pe = ref.Self_Halo_Potent(r[:, 0], r[:, 1], r[:, 2], mf)
+    vs = np.sqrt(np.median(-pe.astype(np.float64))) / r2k  # about half bound
+    v = (vs * rng.standard_normal((len(r), 3))).astype(np.float32)
+    out = dict(pos=r, vel=v, mass=mf, type=typ, self_pe=pe)
+    out["self_flag"], out["self_nb"] = ref.CheckSelfTE(r[:, 0], r[:, 1], r[:, 2], v[:, 0], v[:, 1],
+                                                       v[:, 2], mf, typ)
+    # fewer than 100 members (direct sum) and a member set without stars
+    s = slice(0, 70)
+    vsm = v[s] * np.float32(0.15)
+    out["small_vel"] = vsm
+    out["small_flag"], out["small_nb"] = ref.CheckSelfTE(r[s, 0], r[s, 1], r[s, 2], vsm[:, 0],
+                                                         vsm[:, 1], vsm[:, 2], mf[s], typ[s])
+    out["small_pe"] = ref.Self_Halo_Potent(r[s, 0], r[s, 1], r[s, 2], mf[s])
+    dm = np.full(70, 2, np.int32)
+    out["nostar_flag"], out["nostar_nb"] = ref.CheckSelfTE(r[s, 0], r[s, 1], r[s, 2], vsm[:, 0],
+                                                           vsm[:, 1], vsm[:, 2], mf[s], dm)
+    # a satellite's particles against the host's potential
+    sat = r[1::2][:1200] + np.array([0.02, -0.01, 0.015])
+    vsat = v[1::2][:1200] * np.float32(0.7)
+    msat = mf[1::2][:1200]
+    core6 = np.array([*r.mean(0), *v.mean(0)], np.float32)
+    out.update(ext_pos=sat, ext_vel=vsat, ext_mass=msat, ext_core=core6,
+               ext_pe=ref.External_Halo_Potent(sat[:, 0], sat[:, 1], sat[:, 2], msat, r[:, 0],
+                                               r[:, 1], r[:, 2], mf))
+    out["ext_flag"], out["ext_nb"] = ref.CheckExternalTE(sat[:, 0], sat[:, 1], sat[:, 2],
+                                                         vsat[:, 0], vsat[:, 1], vsat[:, 2], msat,
+                                                         r[:, 0], r[:, 1], r[:, 2], mf, core6)
+    # tidal radius: cores of 0..2500 members, overlapping and far pairs
+    rng = np.random.default_rng(43)
+    sizes = [0, 40, 90, 150, 400, 900, 2000, 2500, 60, 300]
+    centres = [(0.2, 0.2, 0.2), (0.30, 0.30, 0.30), (0.301, 0.302, 0.299), (0.5, 0.2, 0.3),
+               (0.32, 0.28, 0.31), (0.8, 0.8, 0.8), (0.3, 0.3, 0.3), (0.55, 0.25, 0.3),
+               (0.9, 0.1, 0.5), (0.82, 0.78, 0.81)]
+    sigmas = [0.01, 0.004, 0.003, 0.006, 0.008, 0.012, 0.02, 0.025, 0.003, 0.006]
+    tpos, thid = clumps(rng, sizes, centres, sigmas)
+    tmass = 10 ** rng.uniform(7, 8.5, len(tpos))
+    tcore = np.zeros((len(sizes), 6), np.float32)
+    for c in range(len(sizes)):
+        sel = thid == c
+        tcore[c, :3] = tpos[sel].mean(0) if sel.any() else centres[c]
+        tcore[c, 3:] = 30.0 * rng.standard_normal(3)
+    counts = np.array(sizes)
+    score = np.array([c for c in np.argsort(counts, kind="stable") if c != 3], np.int32)  # core 3 unranked
+    rt, nm = ref.AdGetTidalRCenterCore(tpos[:, 0], tpos[:, 1], tpos[:, 2], tmass, thid, tcore, score)
+    out.update(tid_pos=tpos, tid_mass=tmass, tid_haloid=thid, tid_core=tcore, tid_score=score,
+               tid_rtidal=rt, tid_nummem=nm)
+    masses = np.array([1e8, 3.3e9, 1e11, 2.7e12, 1e14, 4.4e15])
+    out.update(bg_mass=masses, bg=np.array([ref.bg_potent(float(m)) for m in masses]))
+    np.savez_compressed(OUT / "bound.npz", **out)
 
 
 if __name__ == "__main__":
