@@ -131,14 +131,7 @@ def run_reference_stage(ref, hb, halos, mesh_rule):
     from galaxyfinder_b200 import batch
     t0 = time.perf_counter()
     for h in halos:
-        a, b = int(hb.pstart[h]), int(hb.pstart[h + 1])
-        p = np.stack([hb.x[a:b], hb.y[a:b], hb.z[a:b]], 1)
-        for ax in range(3):
-            c = p[:, ax]
-            cs = np.where(c < 50.0, c + 100.0, c)
-            if c.max() - c.min() > 50.0 and cs.max() - cs.min() < c.max() - c.min():
-                p[:, ax] = cs
-        p = p - p.min(axis=0)
+        p, a, b = recentred_halo(hb, h)
         m = hb.mass[a:b]
         ref.findsphdensity(p[:, 0], p[:, 1], p[:, 2], m, min(K_NEIGH, b - a))
         mesh, _ = batch.plan_meshes(p.max(0)[None, :], mesh_rule)
@@ -149,6 +142,49 @@ def run_reference_stage(ref, hb, halos, mesh_rule):
         den = ref.gaussian_Smoothing(den, *n3, cell, float(mm["rg"]))
         ref.findDen(p[:, 0], p[:, 1], p[:, 2], den, *n3, o, o, o, cell)
         ref.Self_Halo_Potent(p[:, 0], p[:, 1], p[:, 2], m.astype(np.float32))
+    return time.perf_counter() - t0
+
+
+def recentred_halo(hb, h):
+    """Dump2BP's recentring of one halo after the periodic unwrap (FP64)."""
+    a, b = int(hb.pstart[h]), int(hb.pstart[h + 1])
+    p = np.stack([hb.x[a:b], hb.y[a:b], hb.z[a:b]], 1)
+    for ax in range(3):
+        c = p[:, ax]
+        cs = np.where(c < 50.0, c + 100.0, c)
+        if c.max() - c.min() > 50.0 and cs.max() - cs.min() < c.max() - c.min():
+            p[:, ax] = cs
+    return p - p.min(axis=0), a, b
+
+
+def run_dropin_stage(hb, halos, mesh_rule):
+    """The drop-in path a reference user gets by linking libgf: per halo,
+    findsphdensity + assign_density_TSC + gaussian_Smoothing + findDen +
+    Self_Halo_Potent through the reference signatures with host buffers (one
+    halo per call, copies inside every call).  Inputs are built before the
+    clock starts, as the reference has them in its own arrays.  Returns
+    seconds."""
+    from galaxyfinder_b200 import _lib, batch, dropin
+    prepared = []
+    for h in halos:
+        p, a, b = recentred_halo(hb, h)
+        bp = np.zeros(b - a, _lib.BP_DTYPE)
+        bp["x"], bp["y"], bp["z"] = p[:, 0], p[:, 1], p[:, 2]
+        bp["mass"], bp["type"] = hb.mass[a:b], hb.type[a:b]
+        mesh, _ = batch.plan_meshes(p.max(0)[None, :], mesh_rule)
+        mm = mesh[0]
+        den = np.zeros(dropin.mesh_floats(int(mm["nx"]), int(mm["ny"]), int(mm["nz"])), np.float32)
+        prepared.append((bp, p, hb.mass[a:b].astype(np.float32), mm, den, min(K_NEIGH, b - a)))
+    t0 = time.perf_counter()
+    for bp, p, m32, mm, den, k in prepared:
+        n3 = (int(mm["nx"]), int(mm["ny"]), int(mm["nz"]))
+        o, cell = float(mm["xmin"]), float(mm["cellsize"])
+        dropin.findsphdensity(bp, k)
+        den[:] = 0
+        dropin.assign_density_TSC(bp, *n3, o, o, o, cell, _lib.TYPE_ALL, den=den)
+        dropin.gaussian_Smoothing(den, *n3, cell, float(mm["rg"]))
+        dropin.findDen(bp, den, *n3, o, o, o, cell)
+        dropin.Self_Halo_Potent(p, m32)
     return time.perf_counter() - t0
 
 
@@ -307,6 +343,22 @@ def main():
     e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps)
     e2e_value = total_particles / (e2e_ms / 1e3)
 
+    # ---- plain GPU path: one halo per gf_stage_run call, same kernels,
+    # inputs resident (the batching's own gain), over the whole catalogue
+    views = batch.HaloViews(db, out, K_NEIGH, hb.pstart)
+    views.run(ctx, cfg, halos=range(min(64, hb.nhalo)))
+    torch.cuda.synchronize()
+    barrier()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    views.run(ctx, cfg)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(g0.elapsed_time(g1))
+    plain = {"value": total_particles / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
+             "path": "one halo per gf_stage_run call (device-resident inputs, same kernels)",
+             "batched_over_plain": value / (total_particles / (plain_ms / 1e3))}
+
     # ---- roofline of the dominant kernel
     pk = peaks()
     dom = max(phases, key=phases.get)
@@ -351,6 +403,7 @@ def main():
         "knn_work_per_query": {k[4:]: st[k] / max(hb.n, 1) for k in
                                ("knn_nodes", "knn_batches", "knn_candidates",
                                 "knn_single_inserts", "knn_bitonic_merges")},
+        "plain": plain,
         "gpu_launches": int(launches),
         "clocks": clk,
     })
@@ -362,6 +415,13 @@ def main():
             ref = orc.Reference("fixed")
             halos, npart = reference_sample(hb, args.cpu_budget)
             t = run_reference_stage(ref, hb, halos, mesh_rule)
+            run_dropin_stage(hb, halos[:2], mesh_rule)
+            td = run_dropin_stage(hb, halos, mesh_rule)
+            line["plain"]["dropin"] = {
+                "value": npart / td, "unit": UNIT, "seconds": td,
+                "path": "reference signatures (findsphdensity, assign_density_TSC, "
+                        "gaussian_Smoothing, findDen, Self_Halo_Potent), host buffers, "
+                        "one halo per call, on the cpu_baseline sample"}
             line["cpu_baseline"] = {
                 "value": npart / t, "unit": UNIT, "cores": orc.cpu_threads(), "kind": "reference",
                 "sample": f"{len(halos)} of {hb.nhalo} halos ({npart} particles, seeded random order); "

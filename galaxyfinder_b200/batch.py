@@ -173,6 +173,34 @@ class StageBuffers:
                              ptr(self.penergy), ptr(self.xr), ptr(self.yr), ptr(self.zr))
 
 
+class HaloViews:
+    """Each halo of a batch as a batch of one (device pointers offset into the
+    batch and its outputs): the plain path, one halo per gf_stage_run call."""
+
+    def __init__(self, batch: DeviceBatch, out: StageBuffers, k: int, pstart_host: np.ndarray):
+        ps = np.asarray(pstart_host, np.int64)
+        counts = np.diff(ps)
+        self.one = torch.zeros((batch.nhalo, 2), dtype=torch.int64, device=batch.x.device)
+        self.one[:, 1] = torch.as_tensor(counts, device=batch.x.device)
+        self.views = []
+        kk = max(k, 1)
+        for h in range(batch.nhalo):
+            a, n = int(ps[h]), int(counts[h])
+            b = Batch(1, n, self.one.data_ptr() + 16 * h, batch.x.data_ptr() + 8 * a,
+                      batch.y.data_ptr() + 8 * a, batch.z.data_ptr() + 8 * a,
+                      batch.mass.data_ptr() + 8 * a, batch.type.data_ptr() + 4 * a)
+            o = _lib.StageOut(out.nearindex.data_ptr() + 4 * kk * a, out.dens_sph.data_ptr() + 4 * a,
+                              out.dens_mesh.data_ptr() + 4 * a, out.penergy.data_ptr() + 4 * a,
+                              None, None, None)
+            self.views.append((b, o))
+
+    def run(self, ctx: Context, cfg: _lib.StageConfig, halos=None):
+        L = lib()
+        for h in (range(len(self.views)) if halos is None else halos):
+            b, o = self.views[h]
+            check(L.gf_stage_run(ctx.handle, ctypes.byref(b), ctypes.byref(cfg), ctypes.byref(o), None))
+
+
 def stage_run(ctx: Context, batch: DeviceBatch, cfg: _lib.StageConfig,
               out: StageBuffers | None = None, stats=False):
     """Runs the whole density-and-potential stage on the batch."""
