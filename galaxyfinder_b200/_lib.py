@@ -175,6 +175,14 @@ SIGNATURES = {
     "gf_tree_build": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _INT, ctypes.POINTER(TreeInfo)]),
     "gf_tree_export": (_INT, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "gf_knn_density": (_INT, [_VP, _I32, _I64, _VP, _VP, _INT, _VP, _VP]),
+    "gf_knn_query": (_INT, [_VP, _I32, _I64, _VP, _VP, _INT, _I64, _VP, _VP, _VP]),
+    "gf_knn_density_adjoint": (_INT, [_VP, _I32, _I64, _VP, _VP, _VP, _VP, _INT, _I64, _VP, _VP,
+                                      _VP, _VP, _VP, _VP]),
+    "gf_tsc_adjoint": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP, _VP, _VP, _VP]),
+    "gf_find_den_adjoint": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP, _VP, _VP, _VP,
+                                   _VP]),
+    "gf_mesh_peaks": (_INT, [_VP, _I32, _VP, _VP, _VP, _INT, _F, _I64, _VP, _VP, _VP,
+                             ctypes.POINTER(_I64)]),
     "gf_self_potential": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _I32, _D, _INT, _VP, _VP]),
     "gf_stage_run": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),
                             ctypes.POINTER(StageOut), ctypes.POINTER(StageStats)]),

@@ -137,6 +137,10 @@ int check_device_errors(gf_ctx *ctx) {
             set_status(GF_ETIMEOUT, "a tree walk exceeded its step bound");
             return GF_ETIMEOUT;
         }
+        if (h & GF_ERRBIT_INDEX) {
+            set_status(GF_EINVAL, "an index argument is out of range");
+            return GF_EINVAL;
+        }
         set_status(GF_EDEVICE, "device error word 0x%x", h);
         return GF_EDEVICE;
     }

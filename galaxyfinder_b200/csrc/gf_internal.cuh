@@ -55,6 +55,7 @@ enum : int {
     GF_ERRBIT_TREE = 2,       // tree build ran out of node capacity
     GF_ERRBIT_KNN = 4,        // a kNN query found fewer than k neighbours
     GF_ERRBIT_WALK = 8,       // a tree walk exceeded its step bound
+    GF_ERRBIT_INDEX = 16,     // an index argument (query, neighbour) is out of range
 };
 
 // ---------------------------------------------------------------- workspace

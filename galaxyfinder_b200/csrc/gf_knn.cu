@@ -253,7 +253,8 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
            const float4 *__restrict__ pos_batch, const int32_t *__restrict__ phalo,
            const int64_t *__restrict__ pstart, const int32_t *__restrict__ owner,
            const KnnNode *__restrict__ nodes, int32_t *__restrict__ nearindex,
-           float *__restrict__ dens, int *err, unsigned long long *__restrict__ counters) {
+           float *__restrict__ dens, int *err, unsigned long long *__restrict__ counters,
+           const int32_t *__restrict__ qlist) {
     const int lane = threadIdx.x & 31;
     // work counters: nodes tested, 32-wide leaf batches, candidates that pass
     // the float filter, candidates inserted one by one, bitonic batch merges
@@ -268,7 +269,9 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
         ListState L;
         L.Ld = kInf;
         L.Li = INT_MAX;
-        for (int64_t q = q0; q < q1; q++) {
+        for (int64_t qi = q0; qi < q1; qi++) {
+            // with a query list, row qi of the outputs is tree position qlist[qi]
+            const int64_t q = qlist ? (int64_t)qlist[qi] : qi;
             const int h = phalo[q];
             const int64_t hs = pstart[h], he = pstart[h + 1];
             const int nh = (int)(he - hs);
@@ -325,7 +328,7 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
                 continue;
             }
             // ---- outputs in batch order
-            const int qo = perm[q];
+            const int64_t qo = qlist ? qi : (int64_t)perm[q];
             if (lane < k) nearindex[(int64_t)qo * k + lane] = lane < kk ? (int32_t)(L.Li - hs) : -1;
             // nnost.c:292,415: maxr = sqrtf(maxdist2); W4(sqrtf(d2_j), maxr/2.)
             const float neardist = sqrtf((float)__shfl_sync(0xffffffffu, L.Ld, kk - 1));
@@ -343,24 +346,26 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
 }  // namespace
 
 int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const float4 *pos_batch, int k,
-               int32_t *nearindex, float *dens, unsigned long long *counters) {
+               int32_t *nearindex, float *dens, unsigned long long *counters,
+               const int32_t *qlist, int64_t nq) {
     if (k < 1 || k > 32) {
         set_status(GF_EINVAL, "k = %d: the warp kNN supports 1 <= k <= 32", k);
         return GF_EINVAL;
     }
-    if (t.n <= 0) return GF_OK;
+    const int64_t nquery = qlist ? nq : t.n;
+    if (t.n <= 0 || nquery <= 0) return GF_OK;
     const int block = 256;
-    const int64_t warps_needed = (t.n + kChunk - 1) / kChunk;
+    const int64_t warps_needed = (nquery + kChunk - 1) / kChunk;
     int64_t grid = (warps_needed * 32 + block - 1) / block;
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * 8));
     if (counters)
-        knn_kernel<true><<<(int)grid, block, 0, ctx->stream>>>(t.n, k, t.pos, t.perm, pos_batch, t.phalo,
+        knn_kernel<true><<<(int)grid, block, 0, ctx->stream>>>(nquery, k, t.pos, t.perm, pos_batch, t.phalo,
                                                                pstart, t.owner, t.knn, nearindex, dens,
-                                                               ctx->d_err, counters);
+                                                               ctx->d_err, counters, qlist);
     else
-        knn_kernel<false><<<(int)grid, block, 0, ctx->stream>>>(t.n, k, t.pos, t.perm, pos_batch, t.phalo,
+        knn_kernel<false><<<(int)grid, block, 0, ctx->stream>>>(nquery, k, t.pos, t.perm, pos_batch, t.phalo,
                                                                 pstart, t.owner, t.knn, nearindex, dens,
-                                                                ctx->d_err, nullptr);
+                                                                ctx->d_err, nullptr, qlist);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }

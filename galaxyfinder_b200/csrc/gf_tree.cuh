@@ -25,7 +25,8 @@ struct PotentialParams {
 // pos_batch: the same FP32 positions in batch order (seeds re-read them by
 // batch index).
 int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const float4 *pos_batch, int k,
-               int32_t *nearindex, float *dens, unsigned long long *counters = nullptr);
+               int32_t *nearindex, float *dens, unsigned long long *counters = nullptr,
+               const int32_t *qlist = nullptr, int64_t nq = 0);
 int launch_self_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart,
                           const PotentialParams &pp, float *penergy, float *raw,
                           unsigned long long *counters);

@@ -120,6 +120,25 @@ def config1(seed: int = SEED_BASE + 1, n: int = 131072) -> HaloBatch:
                    {"config": 1, "seed": seed, "r200": r200, "c": c})
 
 
+def config4(seed: int = SEED_BASE + 4, n: int = 10_000_000, nclump: int = 64) -> HaloBatch:
+    """Differentiable-density workload: one Gaussian-mixture halo of n
+    equal-mass (1e8) DM particles in nclump clumps with sigma log-uniform in
+    5-50 kpc/h, log-uniform weights (normalised) and centres uniform in a
+    sphere of radius 0.5 Mpc/h."""
+    rng = np.random.default_rng(seed)
+    centre = 10.0 + rng.random(3) * (BOX - 20.0)
+    sig = np.exp(rng.uniform(np.log(0.005), np.log(0.05), nclump))
+    w = np.exp(rng.uniform(0.0, np.log(100.0), nclump))
+    w /= w.sum()
+    counts = rng.multinomial(n, w)
+    rad = 0.5 * rng.random(nclump) ** (1.0 / 3.0)
+    ctr = centre + _directions(rng, nclump) * rad[:, None]
+    pos = np.concatenate([c + s * rng.standard_normal((k, 3)) for c, s, k in zip(ctr, sig, counts)])
+    pos = pos[rng.permutation(n)]
+    return _finish([pos], [np.full(n, DM_MASS)], [np.full(n, TYPE_DM, np.int32)], rng,
+                   {"config": 4, "seed": seed, "nclump": nclump})
+
+
 def powerlaw_counts(rng, nhalo, nmin, nmax, slope=-1.9):
     """N_p drawn from dN/dN_p ~ N_p^slope on [nmin, nmax] by inverse CDF."""
     a = slope + 1.0

@@ -202,6 +202,32 @@ int gf_gaussian_smooth(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host
 int gf_find_den(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh_dev, const float *den,
                 float *densph);
 
+/* Adjoints (no reference counterpart: the reference has no derivatives).
+ * Gradients are FP64 device arrays that these calls ADD to.
+ *   gf_tsc_adjoint: the deposit of tsc_omp2.c:166 with respect to positions
+ *     and masses, given dL/dden in gden (padded mesh layout); gm may be NULL.
+ *   gf_find_den_adjoint: the interpolation of tsc_omp2.c:40 given dL/drho_p
+ *     in gdens: adds g_p * W to the mesh gradient gden (float, may be NULL)
+ *     and, when den (the interpolated mesh) is given, g_p * dW/dx * den to
+ *     the position gradients.
+ * The Gaussian smoothing of gsmooth.c:14 is self-adjoint (a real, even
+ * filter): gf_gaussian_smooth of a mesh gradient is its adjoint. */
+int gf_tsc_adjoint(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh_dev, const float *gden,
+                   double *gx, double *gy, double *gz, double *gm);
+int gf_find_den_adjoint(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh_dev,
+                        const float *den, const double *gdens, float *gden, double *gx,
+                        double *gy, double *gz);
+
+/* Strict 26-neighbour maxima of every mesh above threshold, in the interior
+ * [margin, n - margin) of each axis (the mesh peak test of nnost.c:1176-1200;
+ * lagFindStellarCore uses margin NCELLBUFF/2 and PEAKTHRESHOLD).  Up to cap
+ * peaks are written (halo, cell offset within the halo's mesh, value) in no
+ * particular order; *npeak receives the number found (may exceed cap). */
+int gf_mesh_peaks(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
+                  const gf_mesh_desc *mesh_dev, const float *den, int margin, float threshold,
+                  int64_t cap, int32_t *out_halo, int64_t *out_cell, float *out_val,
+                  int64_t *npeak);
+
 /* ------------------------------------------------------------------------
  * Centre-of-mass octree (ost.c:532-699 Make_Tree / divide_node, nnost.c:105-254
  * new_Make_Tree_Near), kNN + SPH density (nnost.c:375-422 Find_Near,
@@ -229,6 +255,21 @@ int gf_tree_export(gf_ctx *ctx, void *bh_nodes, void *knn_nodes, float *pos4, in
  * index; halo-local indices, -1 past a halo's size) and W4 density. */
 int gf_knn_density(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
                    const float *pos4_dev, int k, int32_t *nearindex, float *dens);
+/* The same search for the nq particles listed in qidx (batch indices):
+ * row q of nearindex (halo-local indices) and dens belongs to qidx[q]. */
+int gf_knn_query(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                 const float *pos4_dev, int k, int64_t nq, const int64_t *qidx_dev,
+                 int32_t *nearindex, float *dens);
+/* Adjoint of the W4 density rho_i = sum_j W4(|x_i - x_j|, r_k/2)
+ * (nnost.c:536-630) with respect to the FP64 positions x, y, z (batch
+ * order): for each row q (particle qidx[q], or q when qidx is NULL) with its
+ * neighbour list nearindex[q*k ..] (halo-local, from the forward search) and
+ * upstream gradient gdens[q], adds to gx/gy/gz the terms of the pair
+ * distances and of the kernel width h = r_k/2. */
+int gf_knn_density_adjoint(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
+                           const double *x, const double *y, const double *z, int k, int64_t nq,
+                           const int64_t *qidx_dev, const int32_t *nearindex, const double *gdens,
+                           double *gx, double *gy, double *gz);
 /* Self potential of every halo: penergy = phi * potentfact + bg(halo mass)
  * (bg only if add_bg); halos with fewer than ndirect particles are summed
  * directly.  raw (optional) receives phi itself. */

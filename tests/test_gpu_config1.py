@@ -76,10 +76,10 @@ def _library_fp32_smoothing(d, n3, cell, rg):
     a = np.asarray(d, np.float32).reshape(nz, ny, mx)[:, :, :nx]
     kz, ky = np.fft.fftfreq(nz) * nz, np.fft.fftfreq(ny) * ny
     kx = np.arange(nx // 2 + 1)
-    fac = (np.pi * rg / cell) ** 2
+    fac = (np.pi * float(np.float32(float(np.float32(rg)) / cell))) ** 2  # gsmooth.c:14,67
     filt = np.exp(-fac * (kz[:, None, None] ** 2 / nz ** 2 + ky[None, :, None] ** 2 / ny ** 2
                           + kx[None, None, :] ** 2 / nx ** 2)).astype(np.float32)
-    s = sf.irfftn(sf.rfftn(a) * filt, s=(nz, ny, nx)).astype(np.float32)
+    s = sf.irfftn(sf.rfftn(a) * filt, s=(nz, ny, nx), axes=(0, 1, 2)).astype(np.float32)
     full = np.zeros((nz, ny, mx), np.float32)
     full[:, :, :nx] = s
     return full.ravel()
