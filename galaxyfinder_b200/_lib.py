@@ -159,6 +159,7 @@ SIGNATURES = {
     "Self_Halo_Potent": (None, [_INT, _VP, _VP, _VP]),
     "External_Halo_Potent": (None, [_INT, _VP, _VP, _VP, _INT, _VP, _VP]),
     "i_potent_spline": (None, []),
+    "lagFindStellarCore": (None, [_VP, _INT, _INT, _VP, _VP, _VP, _INT, _VP, _INT]),
     "CheckSelfTE": (_INT, [_VP, _INT, _VP, _VP]),
     "CheckExternalTE": (_INT, [_VP, _INT, _VP, _VP, _INT, _VP]),
     "gf_tidal_radius": (_INT, [_VP, _INT, _VP, _INT, _VP, _VP, _INT]),
@@ -196,6 +197,9 @@ def lib() -> ctypes.CDLL:
         if not LIB_PATH.exists():
             raise FileNotFoundError(
                 f"{LIB_PATH} is not built; run `python -m galaxyfinder_b200.build`")
+        # the void drop-ins exit(99) on error like the reference unless
+        # GF_NOEXIT is set; from Python, errors are raised instead
+        os.environ.setdefault("GF_NOEXIT", "1")
         L = ctypes.CDLL(str(LIB_PATH))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name)

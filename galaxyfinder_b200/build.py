@@ -5,7 +5,8 @@
 
 Each translation unit under csrc/ is compiled by nvcc for
 ``arch=compute_100a,code=sm_100a`` with ``-lineinfo``; the objects are
-linked into ``galaxyfinder_b200/libgf.so``.  ``gf_tsc.cu``, ``gf_knn.cu`` and
+linked into ``galaxyfinder_b200/libgf.so`` and archived into
+``galaxyfinder_b200/libgf.a`` (for linking into the reference program).  ``gf_tsc.cu``, ``gf_knn.cu`` and
 ``gf_bound.cu`` are compiled with ``--fmad=false`` because their results must reproduce the
 reference's separately rounded float/double arithmetic bit for bit.
 """
@@ -22,6 +23,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libgf.so"
+ARCHIVE = PKG / "libgf.a"  # the same objects, for linking libgf into the reference program
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NOFMAD = {"gf_tsc.cu", "gf_knn.cu", "gf_bound.cu"}
 
@@ -60,6 +62,10 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    if force or not ARCHIVE.exists() or ARCHIVE.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        if ARCHIVE.exists():
+            ARCHIVE.unlink()
+        subprocess.run(["ar", "rcs", str(ARCHIVE), *map(str, objs)], check=True)
     return LIB
 
 

@@ -342,6 +342,18 @@ __global__ void mesh_peaks_kernel(const gf_mesh_desc *__restrict__ mesh,
 
 }  // namespace
 
+int launch_mesh_peaks(gf_ctx *ctx, int32_t nhalo, int64_t maxcell, const gf_mesh_desc *mesh_dev,
+                      const float *den, int margin, float threshold, int64_t cap, int32_t *out_halo,
+                      int64_t *out_cell, float *out_val, unsigned long long *dcount) {
+    GF_CUDA_TRY(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), ctx->stream));
+    const int64_t gx = std::min<int64_t>((maxcell + 255) / 256, 148 * 8);
+    dim3 grid((unsigned)std::max<int64_t>(gx, 1), (unsigned)nhalo);
+    mesh_peaks_kernel<<<grid, 256, 0, ctx->stream>>>(mesh_dev, den, margin, threshold, cap, out_halo,
+                                                    out_cell, out_val, dcount);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
 }  // namespace gf
 
 using namespace gf;
@@ -458,12 +470,8 @@ int gf_mesh_peaks(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
         maxcell = std::max<int64_t>(maxcell, (int64_t)mesh_host[h].nx * mesh_host[h].ny * mesh_host[h].nz);
     GF_TRY(ctx->tmp[3].reserve(sizeof(unsigned long long)));
     unsigned long long *dcount = ctx->tmp[3].as<unsigned long long>();
-    GF_CUDA_TRY(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), ctx->stream));
-    const int64_t gx = std::min<int64_t>((maxcell + 255) / 256, 148 * 8);
-    dim3 grid((unsigned)std::max<int64_t>(gx, 1), (unsigned)nhalo);
-    mesh_peaks_kernel<<<grid, 256, 0, ctx->stream>>>(mesh_dev, den, margin, threshold, cap, out_halo,
-                                                    out_cell, out_val, dcount);
-    GF_LAUNCH_CHECK();
+    GF_TRY(launch_mesh_peaks(ctx, nhalo, maxcell, mesh_dev, den, margin, threshold, cap, out_halo,
+                             out_cell, out_val, dcount));
     unsigned long long hcount = 0;
     GF_CUDA_TRY(cudaMemcpyAsync(&hcount, dcount, sizeof(hcount), cudaMemcpyDeviceToHost, ctx->stream));
     GF_TRY(check_device_errors(ctx));

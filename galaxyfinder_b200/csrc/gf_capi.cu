@@ -115,6 +115,15 @@ gf_ctx *default_ctx() {
     return c;
 }
 
+void dropin_exit_on_error(int status, const char *who) {
+    if (status == GF_OK || t_status == GF_OK) return;
+    const char *e = getenv("GF_NOEXIT");
+    if (e && *e && strcmp(e, "0") != 0) return;
+    fprintf(stderr, "%s: %s\n", who, t_msg[0] ? t_msg : "libgf error");
+    fflush(stderr);
+    exit(99);
+}
+
 int check_device_errors(gf_ctx *ctx) {
     int h = 0;
     GF_CUDA_TRY(cudaMemcpyAsync(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -534,18 +543,18 @@ extern "C" {
 void assign_density_TSC(SimpleBasicParticleType *bp, int np, float *den, int nx, int ny, int nz,
                         double Xmin, double Ymin, double Zmin, double cellsize, int ptype) {
     clear_status();
-    do_assign_density_TSC(bp, np, den, nx, ny, nz, Xmin, Ymin, Zmin, cellsize, ptype);
+    dropin_exit_on_error(do_assign_density_TSC(bp, np, den, nx, ny, nz, Xmin, Ymin, Zmin, cellsize, ptype), "assign_density_TSC");
 }
 
 void findDen(SimpleBasicParticleType *bp, int np, float *densph, double xmin, double ymin,
              double zmin, double cellsize, float *den, int nx, int ny, int nz) {
     clear_status();
-    do_findDen(bp, np, densph, xmin, ymin, zmin, cellsize, den, nx, ny, nz);
+    dropin_exit_on_error(do_findDen(bp, np, densph, xmin, ymin, zmin, cellsize, den, nx, ny, nz), "findDen");
 }
 
 void gaussian_Smoothing(float *denGrid, int nx, int ny, int nz, double cellsize, float RG) {
     clear_status();
-    do_gaussian_Smoothing(denGrid, nx, ny, nz, cellsize, RG);
+    dropin_exit_on_error(do_gaussian_Smoothing(denGrid, nx, ny, nz, cellsize, RG), "gaussian_Smoothing");
 }
 
 void i_potent_spline(void) {

@@ -177,6 +177,10 @@ gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r);
 
 // volfact of tsc_omp2.c:188 for the reference cell size 0.004 cMpc/h.
 double tsc_volfact();
+// End of a void drop-in entry point: where the reference would print and
+// exit(99), print the status message and exit unless GF_NOEXIT is set in the
+// environment (the Python package sets it and raises instead).
+void dropin_exit_on_error(int status, const char *who);
 // True when volfact is folded into the deposit weights (exact power of two).
 bool volfact_folds(double v);
 

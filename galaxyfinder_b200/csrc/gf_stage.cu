@@ -406,17 +406,18 @@ extern "C" {
 void findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, int Numnear,
                     float *densph) {
     clear_status();
-    do_findsphdensity(bp, np, nearindex, Numnear, densph);
+    dropin_exit_on_error(do_findsphdensity(bp, np, nearindex, Numnear, densph), "findsphdensity");
 }
 
 void Self_Halo_Potent(int np, Vector3d *r, float *mass, float *penergy) {
     clear_status();
     if (np < 0 || (np > 0 && (!r || !mass || !penergy))) {
         set_status(GF_EINVAL, "Self_Halo_Potent: invalid arguments");
+        dropin_exit_on_error(GF_EINVAL, "Self_Halo_Potent");
         return;
     }
     if (np == 0) return;
-    potent_common(np, r, penergy, np, r, mass, true);
+    dropin_exit_on_error(potent_common(np, r, penergy, np, r, mass, true), "Self_Halo_Potent");
 }
 
 void External_Halo_Potent(int nend, Vector3d *r, float *mass, float *penergy, int snp,
@@ -425,6 +426,7 @@ void External_Halo_Potent(int nend, Vector3d *r, float *mass, float *penergy, in
     (void)mass;
     if (nend < 0 || snp < 0 || (nend > 0 && (!r || !penergy)) || (snp > 0 && (!sr || !smass))) {
         set_status(GF_EINVAL, "External_Halo_Potent: invalid arguments");
+        dropin_exit_on_error(GF_EINVAL, "External_Halo_Potent");
         return;
     }
     if (nend == 0) return;
@@ -432,7 +434,7 @@ void External_Halo_Potent(int nend, Vector3d *r, float *mass, float *penergy, in
         for (int i = 0; i < nend; i++) penergy[i] = 0.f;
         return;
     }
-    potent_common(nend, r, penergy, snp, sr, smass, false);
+    dropin_exit_on_error(potent_common(nend, r, penergy, snp, sr, smass, false), "External_Halo_Potent");
 }
 
 }  // extern "C"

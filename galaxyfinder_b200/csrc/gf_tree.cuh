@@ -34,6 +34,11 @@ int launch_external_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pst
                               int64_t ntarget, const float4 *tpos, const int32_t *thalo,
                               const int32_t *ntarget_halo, const PotentialParams &pp,
                               float *penergy, float *raw);
+// Strict 26-neighbour maxima above threshold in the interior of every mesh
+// (gf_adjoint.cu); *dcount (device) receives the number found.
+int launch_mesh_peaks(gf_ctx *ctx, int32_t nhalo, int64_t maxcell, const gf_mesh_desc *mesh_dev,
+                      const float *den, int margin, float threshold, int64_t cap, int32_t *out_halo,
+                      int64_t *out_cell, float *out_val, unsigned long long *dcount);
 const gf_physics &physics();
 double bg_potent(double mvir);
 // Host NFW helpers (get_concentration, get_alpha, gnfw, GetRvir of

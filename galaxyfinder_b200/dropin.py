@@ -147,6 +147,22 @@ def tidal_select(bp, cx, cy, cz, rtidal, plist=None):
     return out[:cnt.value]
 
 
+def lagFindStellarCore(bp, numnear, ptype=_lib.TYPE_ALL, maxnumcore=100000):
+    """nnost.c:991 — (densph, cores (CORE_DTYPE), nearindex (np, numnear) int64).
+    Loaded on its own, libgf has no MergingPeak: more than 10 cores raise."""
+    bp = _bp(bp)
+    n = len(bp)
+    dens = np.zeros(n, np.float32)
+    near = np.zeros((n, numnear), np.int64)
+    cores = np.zeros(max(maxnumcore, 1), _lib.CORE_DTYPE)
+    cptr = _lib.ctypes.c_void_p(cores.ctypes.data)
+    ncore = _lib.ctypes.c_int(0)
+    lib().lagFindStellarCore(ptr(bp), n, numnear, ptr(dens), _lib.ctypes.byref(cptr),
+                             _lib.ctypes.byref(ncore), maxnumcore, ptr(near), ptype)
+    check_last()
+    return dens, cores[:ncore.value].copy(), near
+
+
 def i_potent_spline():
     """force_spline.mod3.c:81 — no table is needed by the GPU kernel."""
     lib().i_potent_spline()

@@ -139,6 +139,50 @@ def config4(seed: int = SEED_BASE + 4, n: int = 10_000_000, nclump: int = 64) ->
                    {"config": 4, "seed": seed, "nclump": nclump})
 
 
+G_KMS = 4.30091e-9  # G in Mpc (km/s)^2 / Msun
+
+
+def galaxy_group(seed: int = SEED_BASE + 6, ndm: int = 20000, nsat: int = 4,
+                 star_frac: float = 0.25) -> HaloBatch:
+    """One FoF halo with galaxies for the whole per-halo pipeline: an NFW host
+    (c = 8) and nsat satellites, each with a compact stellar core (stars at a
+    third of the component's scale radius, masses 1e6-1e7) inside its own NFW
+    dark halo, and isotropic velocities about each component's bulk velocity
+    with the dispersion sqrt(G M / (2 r_half)) of that component, so that the
+    galaxies are bound."""
+    rng = np.random.default_rng(seed)
+    centre = 20.0 + rng.random(3) * (BOX - 40.0)
+    comps = [(1.0, np.zeros(3), np.zeros(3))]
+    for _ in range(nsat):
+        f = 10 ** rng.uniform(-1.3, -0.7)
+        off = _directions(rng, 1)[0] * rng.uniform(0.25, 0.6)
+        comps.append((f, off, 120.0 * rng.standard_normal(3)))
+    ftot = sum(c[0] for c in comps)
+    pos, vel, mass, typ = [], [], [], []
+    mhost = None
+    for f, off, vbulk in comps:
+        nd = max(200, int(ndm * f / ftot))
+        ns = max(60, int(star_frac * nd))
+        mcomp = nd * DM_MASS + ns * 5e6
+        r200 = r200_of_mass(mcomp) * (1.0 if mhost is None else 0.6)
+        mhost = mhost or mcomp
+        sig = np.sqrt(G_KMS * mcomp / (2.0 * 0.4 * r200))
+        p = np.concatenate([nfw_blob(rng, nd, 8.0, r200, centre + off),
+                            nfw_blob(rng, ns, 8.0, r200 / 3.0, centre + off)])
+        pos.append(p)
+        vel.append(vbulk + sig * rng.standard_normal((nd + ns, 3)) / np.sqrt(3.0) * 1.2)
+        mass.append(np.concatenate([np.full(nd, DM_MASS), 10 ** rng.uniform(6, 7, ns)]))
+        typ.append(np.concatenate([np.full(nd, TYPE_DM), np.full(ns, TYPE_STAR)]).astype(np.int32))
+    pos, vel, mass, typ = map(np.concatenate, (pos, vel, mass, typ))
+    perm = rng.permutation(len(pos))
+    pos, vel, mass, typ = _wrap(pos[perm]), vel[perm], mass[perm], typ[perm]
+    n = len(pos)
+    return HaloBatch(x=pos[:, 0].copy(), y=pos[:, 1].copy(), z=pos[:, 2].copy(), vx=vel[:, 0].copy(),
+                     vy=vel[:, 1].copy(), vz=vel[:, 2].copy(), mass=mass, type=typ,
+                     ids=np.arange(n, dtype=np.int64), pstart=np.array([0, n], np.int64),
+                     meta={"seed": seed, "nsat": nsat})
+
+
 def powerlaw_counts(rng, nhalo, nmin, nmax, slope=-1.9):
     """N_p drawn from dN/dN_p ~ N_p^slope on [nmin, nmax] by inverse CDF."""
     a = slope + 1.0

@@ -5,13 +5,15 @@
  * Two layers, both plain C ABI (no C++ or torch types in any signature):
  *
  *  1. Drop-in entry points with the reference's exact C signatures.  A
- *     reference build links libgf ahead of its own objects (or weakens its own
- *     definitions) and the calls from subhalo_den()/lagFindStellarCore() land
- *     here.  They take the reference's host buffers, copy them to the GPU,
- *     run the kernels and copy results back before returning, so no host
- *     pointer is kept across calls (the reference's Memory2.c arena may move
- *     blocks between calls, Memory2.c:173-195).  Errors never call exit():
- *     the status is kept in gf_last_status()/gf_last_error().
+ *     reference build links libgf's objects in place of its own definitions
+ *      and the calls from subhalo_den() land here.  They take
+ *     the reference's host buffers, copy them to the GPU, run the kernels and
+ *     copy results back before returning, so no host pointer is kept across
+ *     calls (the reference's Memory2.c arena may move blocks between calls,
+ *     Memory2.c:173-195).  The status is kept in gf_last_status() /
+ *     gf_last_error(); where the reference prints and calls exit(99), the
+ *     void entry points do the same unless GF_NOEXIT is set in the
+ *     environment.
  *
  *  2. The native batched API (gf_*): device pointers, many halos per call,
  *     stream-ordered, returning an int status.
@@ -81,6 +83,18 @@ void gaussian_Smoothing(float *denGrid, int nx, int ny, int nz, double cellsize,
 /* NewGalFinder/nnost.c:560.  nearindex holds np*Numnear indices into bp. */
 void findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, int Numnear,
                     float *densph);
+/* NewGalFinder/nnost.c:991.  Mesh density (TSC of the ptype particles,
+ * Gaussian smoothing, findDen at every particle -> densph), the mesh peak
+ * cores (*Core, *NumCore; at most maxnumcore before merging) and the kNN of
+ * every particle (nearindex, np*Numnear) on the GPU.  More than 10 cores are
+ * merged by the reference's own MergingPeak (subhaloden.mod6.c:341) and the
+ * core array is resized with its arena Realloc (Memory2.c:217); both are
+ * resolved when libgf is linked into the reference program.  Without
+ * MergingPeak, more than 10 cores is an error (GF_ENOTIMPL); without Realloc
+ * the array keeps its size. */
+void lagFindStellarCore(SimpleBasicParticleType *bp, int np, int Numnear, float *densph,
+                        Coretype **Core, int *NumCore, int maxnumcore, long long *nearindex,
+                        int ptype);
 /* NewGalFinder/subhaloden.mod6.c:1477 */
 void Self_Halo_Potent(int np, Vector3d *r, float *mass, float *penergy);
 /* NewGalFinder/subhaloden.mod6.c:1537 */

@@ -5,7 +5,10 @@
   tree-potential arithmetic.
 * ``Reference`` — oracle/_ref/libgfref_{fixed,asbuilt}.so, the reference's own
   NewGalFinder C compiled from its sources by oracle/Makefile, behind the thin
-  harness in oracle/ref/ref_harness.c.
+  harness in oracle/ref/ref_harness.c; ``Reference("linked")`` is the same
+  reference code with libgf's drop-ins linked in its place (the link recipe
+  of INTEGRATION.md), used to test the drop-in boundary inside the
+  reference's own pipeline.
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use this.
 """
@@ -32,10 +35,13 @@ def _p(a):
 
 def build(ref: bool = True) -> None:
     """Builds the restatement and, when the reference tree is present, the
-    reference libraries (make -C oracle [ref])."""
+    reference libraries (make -C oracle [ref]) and, when libgf.a exists, the
+    reference linked with libgf (make -C oracle linked)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     if ref and REF_SOURCE.exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+        if (HERE.parent / "galaxyfinder_b200" / "libgf.a").exists():
+            subprocess.run(["make", "-s", "-C", str(HERE), "linked"], check=True)
 
 
 class Restatement:
@@ -166,6 +172,7 @@ class Reference:
             L.ref_External_Halo_Potent.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP, _VP, _VP,
                                                    _VP]
             L.ref_tree_potential.argtypes = [_I, _VP, _VP, _VP, _VP, _F, _VP]
+            L.ref_subhalo_den.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]
             L.ref_CheckSelfTE.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]
             L.ref_CheckExternalTE.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP, _VP,
                                               _VP, _VP, _VP, _VP]
@@ -300,6 +307,15 @@ class Reference:
         self.L.ref_AdGetTidalRCenterCore(len(x), _p(x), _p(y), _p(z), _p(mass), _p(hid), nc,
                                          _p(c6), len(sc), _p(sc), _p(rt), _p(nm))
         return rt, nm
+
+    def subhalo_den(self, x, y, z, vx, vy, vz, mass, type_):
+        """subhaloden.mod6.c:2861 on one FoF halo -> (result, p2halo)."""
+        x, y, z, vx, vy, vz, mass = map(self._d, (x, y, z, vx, vy, vz, mass))
+        t = np.ascontiguousarray(type_, np.int32)
+        p2 = np.zeros(len(x), np.int32)
+        r = self.L.ref_subhalo_den(len(x), _p(t), _p(x), _p(y), _p(z), _p(vx), _p(vy), _p(vz),
+                                   _p(mass), _p(p2))
+        return r, p2
 
 
 def ref_available() -> bool:

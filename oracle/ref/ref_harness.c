@@ -327,3 +327,29 @@ int ref_AdGetTidalRCenterCore(int np, const double *x, const double *y, const do
     Free(bp);
     return 0;
 }
+
+/* ---- the reference's per-halo pipeline (subhaloden.mod6.c:2861) ---- */
+int subhalo_den(FoFTPtlStruct *, int, int *); /* lint is int, header.h:74 */
+
+/* Runs subhalo_den on one FoF halo given as arrays (comoving positions in the
+ * periodic box, velocities, masses, types; linking lengths from the masses as
+ * gfind.c does); p2halo receives each particle's galaxy id (NOT_HALO_MEMBER
+ * for none).  Returns subhalo_den's result (the number of galaxies). */
+int ref_subhalo_den(int np, const int *type, const double *x, const double *y, const double *z,
+                    const double *vx, const double *vy, const double *vz, const double *mass,
+                    int *p2halo) {
+    if (!g_ready) return -1;
+    FoFTPtlStruct *rbp = (FoFTPtlStruct *)calloc((size_t)(np > 0 ? np : 1), sizeof(FoFTPtlStruct));
+    for (int i = 0; i < np; i++) {
+        rbp[i].type = (unsigned)type[i];
+        rbp[i].x = x[i]; rbp[i].y = y[i]; rbp[i].z = z[i];
+        rbp[i].vx = vx[i]; rbp[i].vy = vy[i]; rbp[i].vz = vz[i];
+        rbp[i].mass = mass[i];
+        rbp[i].indx = i;
+        /* the FoF linking length of each particle, as gfind.c:49-88 sets it */
+        rbp[i].link02 = 0.2 * pow(mass[i] / 2.7755e11L / omep, 0.33333333333333333333L);
+    }
+    int res = subhalo_den(rbp, np, p2halo);
+    free(rbp);
+    return res;
+}

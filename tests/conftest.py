@@ -2,11 +2,17 @@
 its C ABI; everything else runs on the CPU."""
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 import pytest
+
+# libgf's void drop-ins exit(99) on error like the reference unless
+# GF_NOEXIT is set; tests want the status instead (also for the reference
+# linked with libgf, which never loads the Python package).
+os.environ.setdefault("GF_NOEXIT", "1")
 
 ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = Path(__file__).resolve().parent / "golden"

@@ -1,0 +1,106 @@
+"""The drop-in boundary inside the reference's own code.
+
+oracle/_ref/libgfref_linked.so is the reference's NewGalFinder objects with
+the drop-in symbols weakened and libgf's objects linked in their place (the
+link recipe of INTEGRATION.md), so every call the reference makes to
+lagFindStellarCore, findsphdensity, Self/External_Halo_Potent,
+CheckSelfTE/CheckExternalTE, the TSC/smoothing/findDen routines and
+i_potent_spline lands on the GPU, while MergingPeak, the watershed, the
+tidal radii and the membership logic stay the reference's host C.  The
+tests compare it with the unmodified reference (libgfref_fixed.so) on the
+same inputs."""
+import numpy as np
+import pytest
+
+from galaxyfinder_b200 import _lib, dropin, synth
+from oracle.oracle import Reference
+
+pytestmark = pytest.mark.gpu
+
+# (seed, DM particles, satellites, star fraction): 1e4-1.4e5 particles, the
+# last above the reference's 1e5 switch to its pre-copied kNN path, one with
+# too few stars for the stellar branch of subhalo_den
+GROUPS = [(1, 8000, 3, 0.25), (2, 20000, 5, 0.25), (4, 20000, 4, 0.0005), (5, 120000, 10, 0.2)]
+
+
+@pytest.fixture(scope="module")
+def refs(cuda_device):
+    return Reference("fixed"), Reference("linked")
+
+
+def _rounded(hb):
+    """Recentred positions, rounded to float and back: the identically rounded
+    positions on which neighbour lists must match bit for bit."""
+    p = np.stack([hb.x, hb.y, hb.z], 1)
+    p = p - p.min(0)
+    return p.astype(np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("seed,ndm,nsat,sf", GROUPS)
+def test_lag_find_stellar_core_inside_the_reference(refs, seed, ndm, nsat, sf):
+    ref, lnk = refs
+    hb = synth.galaxy_group(seed=seed, ndm=ndm, nsat=nsat, star_frac=sf)
+    q = _rounded(hb)
+    for ptype in ((_lib.TYPE_ALL,) if sf < 0.01 else (_lib.TYPE_STAR, _lib.TYPE_ALL)):
+        d0, i0, pk0, c0 = ref.lagFindStellarCore(q[:, 0], q[:, 1], q[:, 2], hb.mass, hb.type, 32, ptype)
+        d1, i1, pk1, c1 = lnk.lagFindStellarCore(q[:, 0], q[:, 1], q[:, 2], hb.mass, hb.type, 32, ptype)
+        np.testing.assert_array_equal(i1, i0)  # kNN lists, bit for bit
+        big = d0 > 1e-3 * d0.max()
+        assert np.max(np.abs(d1[big] - d0[big]) / d0[big]) < 2e-6
+        # the same cores after the reference's MergingPeak: peak particle,
+        # position (float copies of the particle's), density to 2e-6
+        o0, o1 = np.argsort(pk0), np.argsort(pk1)
+        np.testing.assert_array_equal(pk1[o1], pk0[o0])
+        np.testing.assert_array_equal(c1[o1, :3], c0[o0, :3])
+        np.testing.assert_allclose(c1[o1, 3], c0[o0, 3], rtol=2e-6)
+        # up to 10 cores keep the mesh scan order (identical); more are merged
+        # and ordered by density by MergingPeak: equal up to the order of
+        # cores whose densities agree within the tolerance
+        if len(pk0) <= 10:
+            np.testing.assert_array_equal(pk1, pk0)
+        else:
+            assert np.all(np.diff(c1[:, 3]) <= 0)
+        moved = pk1 != pk0
+        if moved.any():
+            dd = np.abs(c0[moved, 3] - c1[moved, 3]) / c0[moved, 3]
+            assert dd.max() < 1e-4
+
+
+@pytest.mark.parametrize("seed,ndm,nsat,sf", GROUPS)
+def test_subhalo_den_membership_inside_the_reference(refs, seed, ndm, nsat, sf):
+    """The reference's whole per-halo galaxy finder (subhaloden.mod6.c:2861)
+    with and without libgf: the same galaxies, and the same membership except
+    for the particles whose energy test or density ordering sits within the
+    two implementations' numerical differences (counted)."""
+    ref, lnk = refs
+    hb = synth.galaxy_group(seed=seed, ndm=ndm, nsat=nsat, star_frac=sf)
+    args = (hb.x, hb.y, hb.z, hb.vx, hb.vy, hb.vz, hb.mass, hb.type)
+    r0, m0 = ref.subhalo_den(*args)
+    r1, m1 = lnk.subhalo_den(*args)
+    assert r0 == r1 and r0 >= 3
+    differ = m0 != m1
+    print(f"group seed={seed} n={hb.n}: {r0} galaxies, membership differs for {differ.sum()} particles")
+    assert differ.mean() <= 5e-4
+    for g in range(r0):
+        n0, n1 = np.sum(m0 == g), np.sum(m1 == g)
+        assert abs(n0 - n1) <= max(3, 2e-3 * n0), (g, n0, n1)
+
+
+def test_lag_find_stellar_core_standalone(cuda_device):
+    """libgf loaded on its own: up to 10 cores need no merging and match the
+    reference; more than 10 need the reference's MergingPeak and fail
+    loudly."""
+    hb = synth.galaxy_group(seed=1, ndm=8000, nsat=3, star_frac=0.25)
+    q = _rounded(hb)
+    bp = np.zeros(hb.n, _lib.BP_DTYPE)
+    bp["x"], bp["y"], bp["z"] = q[:, 0], q[:, 1], q[:, 2]
+    bp["mass"], bp["type"] = hb.mass, hb.type
+    dens, cores, near = dropin.lagFindStellarCore(bp, 32, ptype=_lib.TYPE_STAR)
+    ref = Reference("fixed")
+    d0, i0, pk0, c0 = ref.lagFindStellarCore(q[:, 0], q[:, 1], q[:, 2], hb.mass, hb.type, 32, _lib.TYPE_STAR)
+    assert 0 < len(pk0) <= 10
+    np.testing.assert_array_equal(near, i0)
+    np.testing.assert_array_equal(cores["peak"], pk0)
+    np.testing.assert_allclose(cores["density"], c0[:, 3], rtol=2e-6)
+    with pytest.raises(_lib.GFError):
+        dropin.lagFindStellarCore(bp, 32, ptype=_lib.TYPE_ALL)
