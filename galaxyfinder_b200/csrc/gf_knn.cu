@@ -10,7 +10,8 @@
 //     distinct particles bound the true k-th distance from above, so the walk
 //     prunes from its first node;
 //   * the walk expands bottom-up from the query's own node (its subtree, then
-//     each ancestor's loose particles and other children) and stops once the
+//     each ancestor's range minus the subtree already walked: its loose
+//     particles and other children) and stops once the
 //     ball of the bound lies inside the processed subtree's box, so the list
 //     fills with close particles first and the bound tightens early;
 //   * a node is skipped when the lower bound of its box distance exceeds the
@@ -203,13 +204,13 @@ __device__ __forceinline__ void scan_loose(int l0, int l1, const float4 &Q,
 // reads a node's bound with one shuffle and compares it with the current
 // (tightening) bound.
 template <bool COUNT>
-__device__ __forceinline__ void walk_range(int i0, int i1, const float4 &Q,
+__device__ __forceinline__ void walk_range(int i0, int i1, int x0, int x1, const float4 &Q,
                                            const float4 *__restrict__ pos,
                                            const int32_t *__restrict__ perm,
                                            const KnnNode *__restrict__ nodes, ListState &L,
                                            unsigned long long (&ctr)[5]) {
     const int lane = threadIdx.x & 31;
-    int node = i0;
+    int node = i0 == x0 ? x1 : i0;
     while (node < i1) {
         const int wb = node;
         const int j = wb + lane;
@@ -223,6 +224,10 @@ __device__ __forceinline__ void walk_range(int i0, int i1, const float4 &Q,
             lc = nd.lcount;
         }
         while (node < i1 && node - wb < 32) {
+            if (node == x0) {  // the subtree already walked
+                node = x1;
+                continue;
+            }
             const int li = node - wb;
             if (COUNT) ctr[0]++;
             const float nlb = __shfl_sync(0xffffffffu, lb, li);
@@ -308,16 +313,21 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
             // ball of the bound lies inside the box of the processed subtree
             // (a node's box lies inside its octant region, which holds exactly
             // the subtree's particles, so nothing outside can enter the list).
+            // One walk per level: q's own node's subtree, then each
+            // ancestor's whole range except the subtree walked before it
+            // (one call site keeps the kernel's code small).
             int c = owner[q];
             KnnNode C = nodes[c];
-            walk_range<COUNT>(c, C.skip, Q, pos, perm, nodes, L, ctr);
-            while (C.parent >= 0 && !(L.cnt >= kk && ball_inside(Q, L.bd, C))) {
+            int w0 = c, w1 = C.skip, x0 = -1, x1 = -1;
+            while (true) {
+                walk_range<COUNT>(w0, w1, x0, x1, Q, pos, perm, nodes, L, ctr);
+                if (C.parent < 0 || (L.cnt >= kk && ball_inside(Q, L.bd, C))) break;
                 const int a = C.parent;
                 const KnnNode A = nodes[a];
-                if (COUNT) ctr[0]++;
-                scan_loose<COUNT>(A.lstart, A.lstart + A.lcount, Q, pos, perm, L, ctr);
-                walk_range<COUNT>(a + 1, c, Q, pos, perm, nodes, L, ctr);
-                walk_range<COUNT>(C.skip, A.skip, Q, pos, perm, nodes, L, ctr);
+                w0 = a;
+                w1 = A.skip;
+                x0 = c;
+                x1 = C.skip;
                 c = a;
                 C = A;
             }
