@@ -12,7 +12,8 @@ from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "libgf.so"
+# GF_LIBGF selects another build of the library (tune.py times variants this way)
+LIB_PATH = Path(os.environ.get("GF_LIBGF") or Path(__file__).resolve().parent / "libgf.so")
 
 # status codes (gf.h)
 GF_OK, GF_EINVAL, GF_ENOMEM, GF_EDEVICE, GF_ETIMEOUT, GF_ERANGE, GF_ENOTIMPL = range(7)

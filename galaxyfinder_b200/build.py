@@ -12,6 +12,7 @@ reference's separately rounded float/double arithmetic bit for bit.
 """
 from __future__ import annotations
 
+import json
 import os
 import shutil
 import subprocess
@@ -24,6 +25,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libgf.so"
 ARCHIVE = PKG / "libgf.a"  # the same objects, for linking libgf into the reference program
+TUNED = PKG / "tuned.json"  # launch parameters chosen by tune.py (-D flags)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NOFMAD = {"gf_tsc.cu", "gf_knn.cu", "gf_bound.cu"}
 
@@ -33,18 +35,42 @@ def nvcc() -> str:
     return cand
 
 
-def _flags(name: str) -> list[str]:
+def tuned_params() -> dict:
+    """The launch parameters recorded by tune.py (empty: the header defaults)."""
+    if TUNED.exists():
+        return dict(json.loads(TUNED.read_text()).get("params", {}))
+    return {}
+
+
+def _flags(name: str, params: dict | None = None) -> list[str]:
     f = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-O2",
          "-I", str(ROOT / "include"), "-I", str(CSRC), "--expt-relaxed-constexpr"]
     if name in NOFMAD:
         f.append("--fmad=false")
+    f += [f"-D{k}={int(v)}" for k, v in sorted((tuned_params() if params is None else params).items())]
     return f
+
+
+def compile_one(src: Path, obj: Path, params: dict | None = None, verbose: bool = False) -> None:
+    cmd = [nvcc(), *_flags(src.name, params), "-c", str(src), "-o", str(obj)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def link(objs, lib: Path, verbose: bool = False) -> None:
+    cmd = [nvcc(), "-shared", *ARCH, "-o", str(lib), *map(str, objs), "-lcudart"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     sources = sorted(CSRC.glob("*.cu"))
     headers = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
+    if TUNED.exists():
+        headers.append(TUNED)
     newest_header = max((h.stat().st_mtime for h in headers), default=0.0)
     objs = []
     for src in sources:
@@ -53,15 +79,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         stale = force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header)
         if not stale:
             continue
-        cmd = [nvcc(), *_flags(src.name), "-c", str(src), "-o", str(obj)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        compile_one(src, obj, verbose=verbose)
     if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [nvcc(), "-shared", *ARCH, "-o", str(LIB), *map(str, objs), "-lcudart"]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        link(objs, LIB, verbose)
     if force or not ARCHIVE.exists() or ARCHIVE.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         if ARCHIVE.exists():
             ARCHIVE.unlink()

@@ -1,6 +1,8 @@
 // Internal declarations shared by the libgf CUDA translation units.
 #pragma once
 
+#include "gf_tuning.cuh"
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 

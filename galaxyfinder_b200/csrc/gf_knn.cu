@@ -89,7 +89,7 @@ constexpr double kInf = DBL_MAX;
 // positive), so a float test against bound * (1 + kSlack) never rejects a
 // particle or node that the exact FP64 test would keep.
 constexpr float kSlack = 1e-6f;
-constexpr int kChunk = 32;  // consecutive tree-order queries per warp task
+constexpr int kChunk = GF_KNN_CHUNK;  // consecutive tree-order queries per warp task
 
 __device__ __forceinline__ float f_d2(const float4 &a, const float4 &b) {
     const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
@@ -253,7 +253,7 @@ __device__ __forceinline__ bool ball_inside(const float4 &Q, double bd, const Kn
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(GF_KNN_BLOCK, GF_KNN_MINB)
 knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__restrict__ perm,
            const float4 *__restrict__ pos_batch, const int32_t *__restrict__ phalo,
            const int64_t *__restrict__ pstart, const int32_t *__restrict__ owner,
@@ -364,10 +364,10 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
     }
     const int64_t nquery = qlist ? nq : t.n;
     if (t.n <= 0 || nquery <= 0) return GF_OK;
-    const int block = 256;
+    const int block = GF_KNN_BLOCK;
     const int64_t warps_needed = (nquery + kChunk - 1) / kChunk;
     int64_t grid = (warps_needed * 32 + block - 1) / block;
-    grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * 8));
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * (2048 / block)));
     if (counters)
         knn_kernel<true><<<(int)grid, block, 0, ctx->stream>>>(nquery, k, t.pos, t.perm, pos_batch, t.phalo,
                                                                pstart, t.owner, t.knn, nearindex, dens,

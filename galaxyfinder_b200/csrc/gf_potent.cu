@@ -56,7 +56,7 @@ __device__ double bg_potent_dev(double mvir, const PotentialParams &pp) {
     return vc2 * (1 - gc * log(1 + c));
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(GF_BH_BLOCK, GF_BH_MINB)
 bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__restrict__ thalo,
           const int32_t *__restrict__ tout, const float4 *__restrict__ spos,
           const int32_t *__restrict__ root, const int32_t *__restrict__ rend,
@@ -187,9 +187,9 @@ int launch_self_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart,
     halo_bg_kernel<<<t.nhalo, 256, 0, ctx->stream>>>(t.nhalo, pstart, t.pos, pp, nullptr,
                                                      pp.ndirect, bg, direct);
     GF_LAUNCH_CHECK();
-    const int block = 128;
+    const int block = GF_BH_BLOCK;
     int64_t grid = (t.n + block - 1) / block;
-    grid = std::min<int64_t>(grid, 148LL * 16);
+    grid = std::min<int64_t>(grid, 148LL * (2048 / block));
     bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(t.n, t.pos, t.phalo, t.perm, t.pos, t.root,
                                                     t.rend, t.bh, direct, bg, pp, penergy, raw,
                                                     counters);
@@ -209,8 +209,8 @@ int launch_external_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pst
     halo_bg_kernel<<<t.nhalo, 256, 0, ctx->stream>>>(t.nhalo, pstart_src, t.pos, pp, ntarget_halo,
                                                      pp.ndirect, bg, direct);
     GF_LAUNCH_CHECK();
-    const int block = 128;
-    int64_t grid = std::min<int64_t>((ntarget + block - 1) / block, 148LL * 16);
+    const int block = GF_BH_BLOCK;
+    int64_t grid = std::min<int64_t>((ntarget + block - 1) / block, 148LL * (2048 / block));
     bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, nullptr, t.pos, t.root,
                                                     t.rend, t.bh, direct, bg, pp, penergy, raw,
                                                     nullptr);

@@ -321,7 +321,7 @@ __device__ __forceinline__ void fft_filter_ifft(float2 *b0, float2 *b1, int npai
     }
 }
 
-constexpr int kPencils = 32;  // real pencils per FFT tile (16 complex)
+constexpr int kPencils = GF_FFT_PENCILS;  // real pencils per FFT tile (2 per complex pencil)
 
 template <int AXIS, int LOGN>
 __global__ void __launch_bounds__((kPencils / 2) * (1 << LOGN) / 8)

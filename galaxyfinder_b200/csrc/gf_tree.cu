@@ -28,7 +28,7 @@ namespace {
 
 constexpr int kMinCell = 10;          // MIN_CELL_PARTICLE_NUM, tree.h:20
 constexpr double kMinWidth = 1.E-6;   // MINCELLWIDTH, tree.h:18
-constexpr int kBlock = 256;
+constexpr int kBlock = GF_TREE_BLOCK;
 
 // Order-preserving float <-> uint32 map for atomic min/max on any sign.
 __device__ __forceinline__ unsigned fkey(float v) {

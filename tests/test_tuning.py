@@ -1,0 +1,34 @@
+"""CPU: the autotuner's search space respects the kernels' compile-time limits,
+and build.py turns tuned.json into -D flags."""
+import json
+
+from galaxyfinder_b200 import build as B
+from galaxyfinder_b200 import tune as T
+
+
+def _valid(p):
+    assert p["GF_KNN_BLOCK"] % 32 == 0 and p["GF_KNN_BLOCK"] <= 1024
+    assert p["GF_BH_BLOCK"] % 32 == 0 and p["GF_BH_BLOCK"] <= 1024
+    assert p["GF_FFT_PENCILS"] % 2 == 0 and (p["GF_FFT_PENCILS"] // 2) * 512 // 8 <= 1024
+    assert 128 <= p["GF_TREE_BLOCK"] <= 1024
+    for b, m in ((p["GF_KNN_BLOCK"], p["GF_KNN_MINB"]), (p["GF_BH_BLOCK"], p["GF_BH_MINB"])):
+        assert m >= 1 and b * m <= 2048  # resident threads per SM
+
+
+def test_search_space_is_valid():
+    base = dict(T.DEFAULTS)
+    for g in T.GROUPS:
+        for stage in T.stages(g, base):
+            assert stage
+            for ov in stage:
+                _valid(dict(base, **ov))
+
+
+def test_tuned_params_become_flags(tmp_path, monkeypatch):
+    f = tmp_path / "tuned.json"
+    f.write_text(json.dumps({"params": {"GF_KNN_CHUNK": 16, "GF_BH_BLOCK": 64}}))
+    monkeypatch.setattr(B, "TUNED", f)
+    flags = B._flags("gf_knn.cu")
+    assert "-DGF_KNN_CHUNK=16" in flags and "-DGF_BH_BLOCK=64" in flags and "--fmad=false" in flags
+    assert B.tuned_params() == {"GF_KNN_CHUNK": 16, "GF_BH_BLOCK": 64}
+    assert T.variant_name({"GF_KNN_CHUNK": 16}) == "knn_chunk16"
