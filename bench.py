@@ -35,6 +35,10 @@ METRIC = "particles/s, kNN+TSC/FFT+potential; batched FP32 vs plain GPU at ≤1e
 UNIT = "particles/s"
 K_NEIGH = 32
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per particle of
+# each phase's dominant kernel, from one ncu capture of the 256-halo catalogue
+# (201,933 particles); the traffic scales with the particles processed.
+TRAFFIC_PER_PARTICLE = {"knn": (9.466624e6 + 0.251136e6) / 201933}
 
 
 def parse():
@@ -371,9 +375,12 @@ def main():
     roofline = None
     if alg.get(dom):
         achieved = alg[dom] / (phases[dom] / 1e3) / 1e9
+        traffic = TRAFFIC_PER_PARTICLE.get(dom)
         roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"],
-                    "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": None,
-                    "peak_source": pk["source"]}
+                    "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                    "traffic": None if traffic is None else traffic * n,
+                    "traffic_note": "bytes per launch, ncu capture of the 256-halo catalogue scaled by particles",
+                    "algorithmic_bytes": alg[dom], "peak_source": pk["source"]}
     else:
         # dominant phase has no HBM-bound roofline (tree build / FP32 potential walk);
         # report the largest HBM-bound phase instead
