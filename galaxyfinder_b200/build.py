@@ -7,7 +7,7 @@ Each translation unit under csrc/ is compiled by nvcc for
 ``arch=compute_100a,code=sm_100a`` with ``-lineinfo``; the objects are
 linked into ``galaxyfinder_b200/libgf.so`` and archived into
 ``galaxyfinder_b200/libgf.a`` (for linking into the reference program).  ``gf_tsc.cu``, ``gf_knn.cu`` and
-``gf_bound.cu`` are compiled with ``--fmad=false`` because their results must reproduce the
+``gf_bound.cu`` and ``gf_cores.cu`` are compiled with ``--fmad=false`` because their results must reproduce the
 reference's separately rounded float/double arithmetic bit for bit.
 """
 from __future__ import annotations
@@ -27,7 +27,7 @@ LIB = PKG / "libgf.so"
 ARCHIVE = PKG / "libgf.a"  # the same objects, for linking libgf into the reference program
 TUNED = PKG / "tuned.json"  # launch parameters chosen by tune.py (-D flags)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NOFMAD = {"gf_tsc.cu", "gf_knn.cu", "gf_bound.cu"}
+NOFMAD = {"gf_tsc.cu", "gf_knn.cu", "gf_bound.cu", "gf_cores.cu"}
 
 
 def nvcc() -> str:

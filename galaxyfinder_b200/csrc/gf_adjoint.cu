@@ -27,35 +27,6 @@ int grid_for(int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
 }
 
-// TSC weights and their derivatives along one axis: cells i0, i0+1, i0+2 with
-// i0 = nearest - 1 and r = xp - nearest in [-1/2, 1/2]:
-//   W = (1/2 - r)^2 / 2,  3/4 - r^2,  (1/2 + r)^2 / 2   (tsc_omp2.c:335-343)
-struct Axis64 {
-    int64_t i0;
-    double w[3], dw[3];
-};
-
-__device__ __forceinline__ Axis64 tsc_axis64(double pos, double origin, double cell) {
-    Axis64 a;
-    const double xp = (pos - origin) / cell;
-    const double nr = rint(xp);
-    const double r = xp - nr;
-    a.i0 = (int64_t)nr - 1;
-    a.w[0] = 0.5 * (0.5 - r) * (0.5 - r);
-    a.w[1] = 0.75 - r * r;
-    a.w[2] = 0.5 * (0.5 + r) * (0.5 + r);
-    a.dw[0] = (r - 0.5) / cell;
-    a.dw[1] = -2.0 * r / cell;
-    a.dw[2] = (0.5 + r) / cell;
-    return a;
-}
-
-__device__ __forceinline__ bool stencil_in(const Axis64 &ax, const Axis64 &ay, const Axis64 &az,
-                                           const gf_mesh_desc &m) {
-    return ax.i0 >= 0 && ax.i0 + 2 < m.nx && ay.i0 >= 0 && ay.i0 + 2 < m.ny && az.i0 >= 0 &&
-           az.i0 + 2 < m.nz;
-}
-
 // dL/dm_p = volfact sum_c G[c] W_c,  dL/dx_p = volfact m_p sum_c G[c] dW_c/dx
 __global__ void tsc_adjoint_kernel(int64_t n, const double *__restrict__ x,
                                    const double *__restrict__ y, const double *__restrict__ z,

@@ -96,6 +96,89 @@ __global__ void core_assoc_kernel(int64_t n, const double *__restrict__ x,
     }
 }
 
+// Smoothed density at (x, y, z) and its gradient: the TSC-weighted 27-cell
+// gather of findDen (tsc_omp2.c:40-163) with FP64 weights, accumulated in
+// FP64 in the order c (z), b (y), a (x).
+struct DenGrad {
+    double rho, gx, gy, gz;
+    bool ok;
+};
+
+__device__ DenGrad density_and_gradient(const gf_mesh_desc &m, const float *__restrict__ den, double x,
+                                        double y, double z) {
+    DenGrad o{0, 0, 0, 0, false};
+    const Axis64 ax = tsc_axis64(x, m.xmin, m.cellsize);
+    const Axis64 ay = tsc_axis64(y, m.ymin, m.cellsize);
+    const Axis64 az = tsc_axis64(z, m.zmin, m.cellsize);
+    if (!stencil_in(ax, ay, az, m)) return o;
+    const int64_t mx = 2 * (m.nx / 2 + 1);
+    const float *d = den + m.off;
+    for (int c = 0; c < 3; c++) {
+        for (int b = 0; b < 3; b++) {
+            const float *row = d + ax.i0 + mx * ((ay.i0 + b) + (int64_t)m.ny * (az.i0 + c));
+            const double wyz = ay.w[b] * az.w[c];
+            const double dyz = ay.dw[b] * az.w[c];
+            const double ydz = ay.w[b] * az.dw[c];
+            for (int a = 0; a < 3; a++) {
+                const double v = row[a];
+                o.rho += v * ax.w[a] * wyz;
+                o.gx += v * ax.dw[a] * wyz;
+                o.gy += v * ax.w[a] * dyz;
+                o.gz += v * ax.w[a] * ydz;
+            }
+        }
+    }
+    o.ok = true;
+    return o;
+}
+
+// Gradient ascent of each centre on its halo's smoothed density: up to
+// max_steps moves of length step (step_frac * the mesh's smoothing length)
+// along the gradient; a move that does not raise the density is not taken
+// and halves the step.  One thread per centre.
+__global__ void centre_ascent_kernel(int ncentre, const int32_t *__restrict__ halo,
+                                     const gf_mesh_desc *__restrict__ mesh,
+                                     const float *__restrict__ den, double *__restrict__ cx,
+                                     double *__restrict__ cy, double *__restrict__ cz, int max_steps,
+                                     double step_frac, double *__restrict__ rho_out,
+                                     int *__restrict__ moves_out, int *err) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncentre) return;
+    const gf_mesh_desc m = mesh[halo ? halo[c] : 0];
+    double x = cx[c], y = cy[c], z = cz[c];
+    DenGrad e = density_and_gradient(m, den, x, y, z);
+    if (!e.ok) {
+        atomicOr(err, GF_ERRBIT_RANGE);
+        rho_out[c] = 0.0;
+        moves_out[c] = 0;
+        return;
+    }
+    double step = step_frac * m.rg;
+    int moves = 0;
+    for (int it = 0; it < max_steps; it++) {
+        const double gn = sqrt(e.gx * e.gx + e.gy * e.gy + e.gz * e.gz);
+        if (!(gn > 0.0)) break;
+        const double nx = x + step * (e.gx / gn);
+        const double ny = y + step * (e.gy / gn);
+        const double nz = z + step * (e.gz / gn);
+        const DenGrad f = density_and_gradient(m, den, nx, ny, nz);
+        if (f.ok && f.rho > e.rho) {
+            x = nx;
+            y = ny;
+            z = nz;
+            e = f;
+            moves++;
+        } else {
+            step *= 0.5;
+        }
+    }
+    cx[c] = x;
+    cy[c] = y;
+    cz[c] = z;
+    rho_out[c] = e.rho;
+    moves_out[c] = moves;
+}
+
 int do_lag_find_stellar_core(SimpleBasicParticleType *bp, int np, int numnear, float *densph,
                              Coretype **Core, int *NumCore, int maxnumcore, long long *nearindex,
                              int ptype) {
@@ -288,6 +371,25 @@ int do_lag_find_stellar_core(SimpleBasicParticleType *bp, int np, int numnear, f
 using namespace gf;
 
 extern "C" {
+
+int gf_refine_centres(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_dev, const float *den,
+                      int32_t ncentre, const int32_t *halo_dev, double *cx, double *cy, double *cz,
+                      int max_steps, double step_frac, double *rho, int32_t *moves) {
+    clear_status();
+    if (!ctx || nhalo <= 0 || ncentre < 0 || max_steps < 0 || !(step_frac > 0) ||
+        (ncentre > 0 && (!mesh_dev || !den || !cx || !cy || !cz || !rho || !moves ||
+                         (nhalo > 1 && !halo_dev)))) {
+        set_status(GF_EINVAL, "gf_refine_centres: invalid arguments");
+        return GF_EINVAL;
+    }
+    if (ncentre == 0) return GF_OK;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    centre_ascent_kernel<<<(ncentre + 127) / 128, 128, 0, ctx->stream>>>(
+        ncentre, nhalo > 1 ? halo_dev : nullptr, mesh_dev, den, cx, cy, cz, max_steps, step_frac, rho,
+        moves, ctx->d_err);
+    GF_LAUNCH_CHECK();
+    return check_device_errors(ctx);
+}
 
 void lagFindStellarCore(SimpleBasicParticleType *bp, int np, int Numnear, float *densph,
                         Coretype **Core, int *NumCore, int maxnumcore, long long *nearindex,

@@ -149,7 +149,8 @@ def galaxy_group(seed: int = SEED_BASE + 6, ndm: int = 20000, nsat: int = 4,
     third of the component's scale radius, masses 1e6-1e7) inside its own NFW
     dark halo, and isotropic velocities about each component's bulk velocity
     with the dispersion sqrt(G M / (2 r_half)) of that component, so that the
-    galaxies are bound."""
+    galaxies are bound.  meta["component"] is each particle's component
+    (0 = host)."""
     rng = np.random.default_rng(seed)
     centre = 20.0 + rng.random(3) * (BOX - 40.0)
     comps = [(1.0, np.zeros(3), np.zeros(3))]
@@ -158,9 +159,9 @@ def galaxy_group(seed: int = SEED_BASE + 6, ndm: int = 20000, nsat: int = 4,
         off = _directions(rng, 1)[0] * rng.uniform(0.25, 0.6)
         comps.append((f, off, 120.0 * rng.standard_normal(3)))
     ftot = sum(c[0] for c in comps)
-    pos, vel, mass, typ = [], [], [], []
+    pos, vel, mass, typ, comp = [], [], [], [], []
     mhost = None
-    for f, off, vbulk in comps:
+    for ic, (f, off, vbulk) in enumerate(comps):
         nd = max(200, int(ndm * f / ftot))
         ns = max(60, int(star_frac * nd))
         mcomp = nd * DM_MASS + ns * 5e6
@@ -173,14 +174,15 @@ def galaxy_group(seed: int = SEED_BASE + 6, ndm: int = 20000, nsat: int = 4,
         vel.append(vbulk + sig * rng.standard_normal((nd + ns, 3)) / np.sqrt(3.0) * 1.2)
         mass.append(np.concatenate([np.full(nd, DM_MASS), 10 ** rng.uniform(6, 7, ns)]))
         typ.append(np.concatenate([np.full(nd, TYPE_DM), np.full(ns, TYPE_STAR)]).astype(np.int32))
-    pos, vel, mass, typ = map(np.concatenate, (pos, vel, mass, typ))
+        comp.append(np.full(nd + ns, ic, np.int32))
+    pos, vel, mass, typ, comp = map(np.concatenate, (pos, vel, mass, typ, comp))
     perm = rng.permutation(len(pos))
-    pos, vel, mass, typ = _wrap(pos[perm]), vel[perm], mass[perm], typ[perm]
+    pos, vel, mass, typ, comp = _wrap(pos[perm]), vel[perm], mass[perm], typ[perm], comp[perm]
     n = len(pos)
     return HaloBatch(x=pos[:, 0].copy(), y=pos[:, 1].copy(), z=pos[:, 2].copy(), vx=vel[:, 0].copy(),
                      vy=vel[:, 1].copy(), vz=vel[:, 2].copy(), mass=mass, type=typ,
                      ids=np.arange(n, dtype=np.int64), pstart=np.array([0, n], np.int64),
-                     meta={"seed": seed, "nsat": nsat})
+                     meta={"seed": seed, "nsat": nsat, "component": comp})
 
 
 def powerlaw_counts(rng, nhalo, nmin, nmax, slope=-1.9):

@@ -232,6 +232,18 @@ int gf_find_den_adjoint(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh
                         const float *den, const double *gdens, float *gden, double *gx,
                         double *gy, double *gz);
 
+/* Galaxy-centre refinement (no reference counterpart; compared with the
+ * search of GalCenter/find_centers.c:25-104): gradient ascent of each centre
+ * (cx, cy, cz: FP64 device arrays, in the frame of its halo's mesh, updated
+ * in place) on that halo's smoothed density den (halo_dev[c]; may be NULL
+ * for one halo): up to max_steps moves of step_frac times the mesh's
+ * smoothing length along the gradient; a move that does not raise the
+ * density is not taken and halves the step.  rho receives the final density
+ * and moves the number of moves taken.  One launch for all centres. */
+int gf_refine_centres(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_dev, const float *den,
+                      int32_t ncentre, const int32_t *halo_dev, double *cx, double *cy, double *cz,
+                      int max_steps, double step_frac, double *rho, int32_t *moves);
+
 /* Strict 26-neighbour maxima of every mesh above threshold, in the interior
  * [margin, n - margin) of each axis (the mesh peak test of nnost.c:1176-1200;
  * lagFindStellarCore uses margin NCELLBUFF/2 and PEAKTHRESHOLD).  Up to cap

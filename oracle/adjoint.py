@@ -15,9 +15,14 @@ that central finite differences with h = 1e-6 are meaningful:
   given neighbour list (r_k = the largest distance in the list);
 * ``*_grad`` — the analytic gradients of the above (product rule over the
   stencil; W4's r and h derivatives), the "plain FP64 reference gradient";
-* ``fd_*`` — central finite differences of the same FP64 functions.
+* ``fd_*`` — central finite differences of the same FP64 functions;
+* ``centre_ascent`` — the gradient ascent of galaxy centres on a smoothed
+  mesh, in the operation order of the GPU kernel (gf_cores.cu), so the two
+  agree bit for bit on the same mesh.
 """
 from __future__ import annotations
+
+import math
 
 import numpy as np
 
@@ -262,3 +267,50 @@ def fd_knn_term(pos, qidx, nbr, parts, h=1e-6):
             d2[n, a] = (vals[2] - vals[-2]) / (4 * h)
             kink[n, a] = crossed
     return d1, d2, kink
+
+
+def density_and_gradient(S, mesh, x):
+    """Smoothed density at x (3,) and its gradient: FP64 TSC weights, sums in
+    the order z, y, x of the 27 cells; None outside the mesh."""
+    S = np.asarray(S, np.float32).reshape(mesh.nz, mesh.ny, mesh.mx)
+    ax = [_axis(np.array([x[a]]), mesh.o[a], mesh.cell) for a in range(3)]
+    (i0, wx, dx), (j0, wy, dy), (k0, wz, dz) = ax
+    i0, j0, k0 = int(i0[0]), int(j0[0]), int(k0[0])
+    if i0 < 0 or i0 + 2 >= mesh.nx or j0 < 0 or j0 + 2 >= mesh.ny or k0 < 0 or k0 + 2 >= mesh.nz:
+        return None
+    wx, wy, wz, dx, dy, dz = (a[0].tolist() for a in (wx, wy, wz, dx, dy, dz))
+    rho = gx = gy = gz = 0.0
+    for c in range(3):
+        for b in range(3):
+            wyz, dyz, ydz = wy[b] * wz[c], dy[b] * wz[c], wy[b] * dz[c]
+            for a in range(3):
+                v = float(S[k0 + c, j0 + b, i0 + a])
+                rho += v * wx[a] * wyz
+                gx += v * dx[a] * wyz
+                gy += v * wx[a] * dyz
+                gz += v * wx[a] * ydz
+    return rho, gx, gy, gz
+
+
+def centre_ascent(S, mesh, start, max_steps=20, step_frac=0.1):
+    """(centre (3,), density, moves): up to max_steps moves of step_frac *
+    R_G along the gradient; a move that does not raise the density is not
+    taken and halves the step."""
+    x = [float(v) for v in start]
+    e = density_and_gradient(S, mesh, x)
+    if e is None:
+        raise ValueError("start outside the mesh")
+    step = step_frac * mesh.rg
+    moves = 0
+    for _ in range(max_steps):
+        gn = math.sqrt(e[1] * e[1] + e[2] * e[2] + e[3] * e[3])
+        if not gn > 0.0:
+            break
+        nx = [x[a] + step * (e[1 + a] / gn) for a in range(3)]
+        f = density_and_gradient(S, mesh, nx)
+        if f is not None and f[0] > e[0]:
+            x, e = nx, f
+            moves += 1
+        else:
+            step *= 0.5
+    return np.array(x), e[0], moves

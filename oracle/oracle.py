@@ -318,6 +318,36 @@ class Reference:
         return r, p2
 
 
+class GalCenterSearch:
+    """GalCenter's own centre search (find_centers.c:25-175), from
+    oracle/_ref/libgalcenter.so."""
+    _lib = None
+
+    def __init__(self, arena_mb: int = 1024):
+        if GalCenterSearch._lib is None:
+            path = REF_DIR / "libgalcenter.so"
+            if not path.exists():
+                if REF_SOURCE.exists():
+                    build(ref=True)
+                else:
+                    raise FileNotFoundError(f"{path} was not built (reference tree absent)")
+            L = ctypes.CDLL(str(path))
+            L.gc_init.argtypes = [ctypes.c_longlong]
+            L.gc_find_centers.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP]
+            if L.gc_init(arena_mb) != 0:
+                raise RuntimeError("GalCenter arena allocation failed")
+            GalCenterSearch._lib = L
+        self.L = GalCenterSearch._lib
+
+    def find_centers(self, x, y, z, mass, type_):
+        """-> (stellar centre (x, y, z, R), dark-matter centre (x, y, z, R))."""
+        x, y, z, m = (np.ascontiguousarray(a, np.float64) for a in (x, y, z, mass))
+        t = np.ascontiguousarray(type_, np.int32)
+        out = np.zeros(8)
+        self.L.gc_find_centers(len(x), _p(t), _p(x), _p(y), _p(z), _p(m), _p(out))
+        return out[:4], out[4:]
+
+
 def ref_available() -> bool:
     return (REF_DIR / "libgfref_fixed.so").exists() or REF_SOURCE.exists()
 
