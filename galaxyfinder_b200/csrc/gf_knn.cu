@@ -5,10 +5,12 @@
 // the k closest particles, self included.  Here one warp serves one query at
 // a time, walking a chunk of consecutive tree-order queries:
 //   * the sorted list (k <= 32) lives in registers, entry j in lane j;
-//   * the bound starts at the k-th closest of the previous query's list (or,
-//     for the first query of a chunk, of the 32 tree-order neighbours): any k
-//     distinct particles bound the true k-th distance from above, so the walk
-//     prunes from its first node;
+//   * the list starts as the k closest of the previous query's list (or,
+//     for the first query of a chunk, of the 32 tree-order neighbours), with
+//     distances recomputed: any k distinct particles bound the true k-th
+//     distance from above, so the walk prunes from its first node, and the
+//     walk skips the seeds (a per-warp set in shared memory) so that only new
+//     particles are merged;
 //   * the walk expands bottom-up from the query's own node (its subtree, then
 //     each ancestor's range minus the subtree already walked: its loose
 //     particles and other children) and stops once the
@@ -167,7 +169,37 @@ struct ListState {
     int kk;     // neighbours wanted
     double bd;  // bound: accept keys <= (bd, bi)
     int bi;
+    int *seeded;  // this warp's set of the seeded list entries (shared memory)
 };
+
+// Per-warp open-addressing set (64 slots, -1 = empty) of the batch indices
+// the list was seeded with; at most 32 entries, so every probe sequence ends
+// within the table.
+constexpr int kSetSlots = 64;
+
+__device__ __forceinline__ unsigned set_slot(int id) {
+    return ((unsigned)id * 2654435761u) >> 26;  // 6 bits
+}
+
+__device__ __forceinline__ void set_insert(int *set, int id) {
+    unsigned h = set_slot(id);
+    for (int t = 0; t < kSetSlots; t++) {
+        const int old = atomicCAS(set + h, -1, id);
+        if (old == -1 || old == id) return;
+        h = (h + 1) & (kSetSlots - 1);
+    }
+}
+
+__device__ __forceinline__ bool set_contains(const int *set, int id) {
+    unsigned h = set_slot(id);
+    for (int t = 0; t < kSetSlots; t++) {
+        const int v = set[h];
+        if (v == id) return true;
+        if (v == -1) return false;
+        h = (h + 1) & (kSetSlots - 1);
+    }
+    return false;
+}
 
 template <bool COUNT>
 __device__ __forceinline__ void scan_loose(int l0, int l1, const float4 &Q,
@@ -185,7 +217,8 @@ __device__ __forceinline__ void scan_loose(int l0, int l1, const float4 &Q,
             if (f_d2(Q, S) <= (float)L.bd * (1.f + kSlack)) {
                 cd = exact_d2(Q, S);
                 ci = perm[jj];
-                acc = !key_lt(L.bd, L.bi, cd, ci);  // (cd, ci) <= (bd, bi)
+                // (cd, ci) <= (bd, bi), and not already in the list as a seed
+                acc = !key_lt(L.bd, L.bi, cd, ci) && !set_contains(L.seeded, ci);
             }
         }
         const unsigned mask = __ballot_sync(0xffffffffu, acc);
@@ -261,8 +294,14 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
            float *__restrict__ dens, int *err, unsigned long long *__restrict__ counters,
            const int32_t *__restrict__ qlist) {
     const int lane = threadIdx.x & 31;
-    // work counters: nodes tested, 32-wide leaf batches, candidates that pass
-    // the float filter, candidates inserted one by one, bitonic batch merges
+    __shared__ int seeded_set[GF_KNN_BLOCK / 32][kSetSlots];
+    int *seeded = seeded_set[threadIdx.x >> 5];
+    seeded[lane] = -1;
+    seeded[lane + 32] = -1;
+    __syncwarp();
+    // work counters: nodes tested, 32-wide leaf batches, candidates accepted
+    // (new and within the bound), candidates inserted one by one, bitonic
+    // batch merges
     unsigned long long ctr[5] = {0, 0, 0, 0, 0};
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -282,8 +321,12 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
             const int nh = (int)(he - hs);
             const int kk = min(k, nh);
             const float4 Q = pos[q];
-            // ---- seed bound: the kk-th closest of the previous query's list
-            // (same halo) or of the 32 tree-order neighbours of q
+            // ---- seed: the list starts as the kk closest of the previous
+            // query's list (same halo; distances recomputed) or of the 32
+            // tree-order neighbours of q, which also bounds the walk from its
+            // first node (kk distinct particles bound the true kk-th
+            // distance).  The seeds are remembered so that the walk does not
+            // insert them twice.
             double d = kInf;
             int id = INT_MAX;
             if (prev_ok && prev_h == h) {
@@ -302,12 +345,15 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
                 }
             }
             warp_sort(d, id);
+            L.Ld = lane < kk ? d : kInf;
+            L.Li = lane < kk ? id : INT_MAX;
             L.bd = __shfl_sync(0xffffffffu, d, kk - 1);
             L.bi = __shfl_sync(0xffffffffu, id, kk - 1);
-            L.Ld = kInf;
-            L.Li = INT_MAX;
-            L.cnt = 0;
+            L.cnt = kk;
             L.kk = kk;
+            L.seeded = seeded;
+            if (lane < kk) set_insert(seeded, id);
+            __syncwarp();
             // ---- bottom-up expanding walk: q's own node's subtree first, then
             // each ancestor's loose particles and other children, until the
             // ball of the bound lies inside the box of the processed subtree
@@ -331,6 +377,9 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
                 c = a;
                 C = A;
             }
+            seeded[lane] = -1;
+            seeded[lane + 32] = -1;
+            __syncwarp();
             prev_h = h;
             prev_ok = L.cnt >= kk;
             if (L.cnt < kk) {
