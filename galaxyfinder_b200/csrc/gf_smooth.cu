@@ -347,19 +347,36 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
     else { base = m.off + t.base + mx * (int64_t)t.other; pstride = 1; sstride = (int)(mx * m.ny); }
     const float *gsrc = den + base;
     const int npen2 = 2 * npair;  // pencils held, the last one zero when npen is odd
+    // All of a thread's loads are issued before any is stored to shared
+    // memory (a fixed count per thread, unrolled), so each warp keeps them
+    // all in flight.
+    constexpr int NT = (kPencils / 2) * N / 8;  // threads per tile
     if (AXIS == 0) {  // rows: consecutive threads walk along a row
-        for (int e = threadIdx.x; e < npen2 * N; e += blockDim.x) {
+        constexpr int PER = kPencils * N / NT;
+        float v[PER];
+#pragma unroll
+        for (int r = 0; r < PER; r++) {
+            const int e = threadIdx.x + r * NT;
             const int p = e >> LOGN, s = e & (N - 1);
-            const float v = p < t.npen ? gsrc[p * pstride + s] : 0.f;
-            fa[2 * L::at(p >> 1, s) + (p & 1)] = v;
+            v[r] = p < t.npen ? gsrc[p * pstride + s] : 0.f;
+        }
+#pragma unroll
+        for (int r = 0; r < PER; r++) {
+            const int e = threadIdx.x + r * NT;
+            const int p = e >> LOGN, s = e & (N - 1);
+            fa[2 * L::at(p >> 1, s) + (p & 1)] = v[r];
         }
     } else {  // columns: lane = pencil (consecutive x), warps step along the axis
+        constexpr int NW = NT / 32;
+        constexpr int PER = N / NW;
         const int p = threadIdx.x & 31;
+        const int w = threadIdx.x >> 5;
         if (p < npen2) {
-            for (int s = threadIdx.x >> 5; s < N; s += blockDim.x >> 5) {
-                const float v = p < t.npen ? gsrc[p + s * sstride] : 0.f;
-                fa[2 * L::at(p >> 1, s) + (p & 1)] = v;
-            }
+            float v[PER];
+#pragma unroll
+            for (int r = 0; r < PER; r++) v[r] = p < t.npen ? gsrc[p + (w + r * NW) * sstride] : 0.f;
+#pragma unroll
+            for (int r = 0; r < PER; r++) fa[2 * L::at(p >> 1, w + r * NW) + (p & 1)] = v[r];
         }
     }
     __syncthreads();
