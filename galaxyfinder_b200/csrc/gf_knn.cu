@@ -230,12 +230,16 @@ __device__ __forceinline__ void scan_loose(int l0, int l1, const float4 &Q,
     }
 }
 
-// Visits the preorder nodes [i0, i1) with pruning: a node whose box lies
-// beyond the bound skips its subtree, otherwise its loose particles are
-// scanned and the walk continues at its first child.  The nodes are read 32
-// at a time, one per lane, with their box lower bounds; the serial walk then
-// reads a node's bound with one shuffle and compares it with the current
-// (tightening) bound.
+// Visits the preorder nodes [i0, i1) except the subtree [x0, x1), with
+// pruning: a node whose box lies beyond the bound hides its subtree (the
+// preorder range up to its skip index); every other node's loose particles
+// are scanned.  The nodes are read 32 at a time, one per lane.  Which of them
+// lie inside a subtree hidden by an earlier node of the window is a prefix
+// maximum of the hidden ranges' ends over the lanes (five shuffles), so the
+// serial part only steps through the visible nodes that hold loose
+// particles, each rechecked against the current (tightening) bound.  A
+// child's box lies inside its parent's, so the recheck prunes exactly what
+// skipping a subtree hidden later would have pruned.
 template <bool COUNT>
 __device__ __forceinline__ void walk_range(int i0, int i1, int x0, int x1, const float4 &Q,
                                            const float4 *__restrict__ pos,
@@ -243,36 +247,50 @@ __device__ __forceinline__ void walk_range(int i0, int i1, int x0, int x1, const
                                            const KnnNode *__restrict__ nodes, ListState &L,
                                            unsigned long long (&ctr)[5]) {
     const int lane = threadIdx.x & 31;
-    int node = i0 == x0 ? x1 : i0;
-    while (node < i1) {
-        const int wb = node;
+    int wb = i0;
+    while (wb < i1) {
         const int j = wb + lane;
+        const bool valid = j < i1;
         float lb = __int_as_float(0x7f800000);  // +inf: beyond the range
         int skip = 0, l0 = 0, lc = 0;
-        if (j < i1) {
+        if (valid) {
             const KnnNode nd = nodes[j];
             lb = f_box_lb2(Q, nd);
             skip = nd.skip;
             l0 = nd.lstart;
             lc = nd.lcount;
         }
-        while (node < i1 && node - wb < 32) {
-            if (node == x0) {  // the subtree already walked
-                node = x1;
-                continue;
-            }
-            const int li = node - wb;
-            if (COUNT) ctr[0]++;
+        // hidden: beyond the bound at the window's start, or the excluded subtree
+        bool hides = valid && lb > (float)L.bd * (1.f + kSlack);
+        if (j == x0) {
+            hides = true;
+            skip = x1;
+        }
+        int cover = hides ? skip : 0;  // inclusive prefix max of the hidden ranges' ends
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, cover, off);
+            if (lane >= off) cover = max(cover, o);
+        }
+        int before = __shfl_up_sync(0xffffffffu, cover, 1);
+        if (lane == 0) before = 0;
+        const bool visible = valid && before <= j;
+        if (COUNT) {
+            const unsigned vm = __ballot_sync(0xffffffffu, visible);
+            if (lane == 0) ctr[0] += __popc(vm);
+        }
+        unsigned todo = __ballot_sync(0xffffffffu, visible && !hides && lc > 0);
+        while (todo) {
+            const int li = __ffs(todo) - 1;
+            todo &= todo - 1;
             const float nlb = __shfl_sync(0xffffffffu, lb, li);
-            if (nlb > (float)L.bd * (1.f + kSlack)) {
-                node = __shfl_sync(0xffffffffu, skip, li);
-                continue;
-            }
+            if (nlb > (float)L.bd * (1.f + kSlack)) continue;
             const int s0 = __shfl_sync(0xffffffffu, l0, li);
             const int sc = __shfl_sync(0xffffffffu, lc, li);
             scan_loose<COUNT>(s0, s0 + sc, Q, pos, perm, L, ctr);
-            node = node + 1;
         }
+        // the next window starts past this one and past every hidden range
+        wb = max(wb + 32, __shfl_sync(0xffffffffu, cover, 31));
     }
 }
 
