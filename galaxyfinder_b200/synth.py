@@ -120,6 +120,38 @@ def config1(seed: int = SEED_BASE + 1, n: int = 131072) -> HaloBatch:
                    {"config": 1, "seed": seed, "r200": r200, "c": c})
 
 
+def config3(seed: int = SEED_BASE + 3, n: int = 50_000_000, nsub: int = 300,
+            star_frac: float = 0.1) -> HaloBatch:
+    """Single massive cluster: n particles, NFW c = 4, r200 = 2 Mpc/h, nsub
+    subhalos with masses from dN/dm ~ m^-1.9 on [1e-5, 1e-2] of the host
+    (NFW, c = 8, r200 scaled as m^(1/3), centred within r200), stars at
+    star_frac by number (masses 1e6-1e7, concentrated x3 in radius); the
+    remaining particles share the host mass."""
+    rng = np.random.default_rng(seed)
+    r200, c = 2.0, 4.0
+    mhost = 200.0 * RHO_C * 4.0 / 3.0 * np.pi * r200 ** 3
+    centre = 10.0 + rng.random(3) * (BOX - 20.0)
+    fr = powerlaw_counts(rng, nsub, 1.0, 1e3).astype(float) * 1e-5
+    nsubp = np.maximum((fr * n).astype(np.int64), 10)
+    nhostp = n - int(nsubp.sum())
+    parts = [nfw_blob(rng, nhostp, c, r200, centre)]
+    rs = r200 * rng.random(nsub) ** (1.0 / 3.0)
+    ctrs = centre + _directions(rng, nsub) * rs[:, None]
+    for k, f in enumerate(fr):
+        parts.append(nfw_blob(rng, int(nsubp[k]), 8.0, r200 * f ** (1.0 / 3.0), ctrs[k]))
+    pos = np.concatenate(parts)
+    typ = np.where(rng.random(n) < star_frac, TYPE_STAR, TYPE_DM).astype(np.int32)
+    st = typ == TYPE_STAR
+    # stars three times more concentrated about their component's centre
+    owner = np.repeat(np.arange(nsub + 1), [nhostp] + nsubp.tolist())
+    cen = np.concatenate([centre[None, :], ctrs])[owner]
+    pos[st] = cen[st] + (pos[st] - cen[st]) / 3.0
+    mass = np.where(st, 10 ** rng.uniform(6, 7, n), mhost / n)
+    perm = rng.permutation(n)
+    return _finish([_wrap(pos[perm])], [mass[perm]], [typ[perm]], rng,
+                   {"config": 3, "seed": seed, "r200": r200, "c": c, "nsub": nsub})
+
+
 def config4(seed: int = SEED_BASE + 4, n: int = 10_000_000, nclump: int = 64) -> HaloBatch:
     """Differentiable-density workload: one Gaussian-mixture halo of n
     equal-mass (1e8) DM particles in nclump clumps with sigma log-uniform in

@@ -1,0 +1,133 @@
+"""The single massive cluster at full size: 5e7 particles (NFW c = 4,
+r200 = 2 Mpc/h, 300 subhalos, 10 % stars), k = 32, a fixed 512^3 TSC mesh
+with Gaussian smoothing of 2 cells, Barnes-Hut at the reference's
+theta^2 = 0.5 and at theta = 0.5 (theta^2 = 0.25).  The oracle checks a seeded
+sample of particles: exact kNN lists (a k-d tree over all 5e7 FP32-rounded
+positions, candidates re-ranked with the kernel's exact FP64 distance and
+index order), SPH densities, the mesh density against an FP64 TSC -> FP64
+FFT smoothing -> findDen chain, and the potential against an FP64 walk of the
+same tree; errors against an FP64 direct sum are printed."""
+import numpy as np
+import pytest
+import torch
+
+from galaxyfinder_b200 import _lib, batch, dropin, synth
+from oracle import adjoint as A
+
+pytestmark = pytest.mark.gpu
+
+NSAMPLE = 2000
+
+
+@pytest.fixture(scope="module")
+def c3(cuda_device):
+    hb = synth.config3()
+    ctx = batch.Context(0)
+    db = batch.DeviceBatch.from_halobatch(hb)
+    rule = batch.mesh_rule(mode=_lib.MESH_FIXED, nfixed=512, rg=2.0, rg_in_cells=True)
+    cfg = batch.stage_config(mesh=rule, knn_k=32)
+    out, st = batch.stage_run(ctx, db, cfg, stats=True)
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(7)
+    sample = np.sort(rng.choice(hb.n, NSAMPLE, replace=False))
+    res = dict(hb=hb, st=st, rule=rule, sample=sample,
+               xr=np.stack([out.xr.cpu().numpy(), out.yr.cpu().numpy(), out.zr.cpu().numpy()], 1),
+               near=out.nearindex[torch.as_tensor(sample, device=out.nearindex.device)].cpu().numpy(),
+               dens_sph=out.dens_sph.cpu().numpy()[sample], dens_mesh=out.dens_mesh.cpu().numpy(),
+               penergy=out.penergy.cpu().numpy()[sample])
+    nn = st["nnode"]
+    res["bh"] = np.zeros(nn, _lib.BH_NODE_DTYPE)
+    res["tpos"] = np.zeros((hb.n, 4), np.float32)
+    res["root"] = np.zeros(1, np.int32)
+    res["rend"] = np.zeros(1, np.int32)
+    _lib.check(_lib.lib().gf_tree_export(ctx.handle, _lib.ptr(res["bh"]), None, _lib.ptr(res["tpos"]), None,
+                                         _lib.ptr(res["root"]), _lib.ptr(res["rend"])))
+    del out, db
+    res["ctx"] = ctx
+    yield res
+    ctx.close()
+
+
+def test_c3_knn_and_sph_density(c3, restatement):
+    from scipy.spatial import cKDTree
+    q = c3["xr"].astype(np.float32).astype(np.float64)
+    s = c3["sample"]
+    tree = cKDTree(q, balanced_tree=False, compact_nodes=False)
+    _, cand = tree.query(q[s], k=48, workers=-1)
+    got = c3["near"]
+    d2_all = np.empty((len(s), 32))
+    for r, i in enumerate(s):
+        c = cand[r]
+        d = q[c] - q[i]
+        d2 = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+        order = np.lexsort((c, d2))
+        assert d2[order[31]] < d2[order[47]]  # the 48 candidates cover the 32nd
+        np.testing.assert_array_equal(got[r], c[order[:32]])
+        d2_all[r] = d2[order[:32]]
+    np.testing.assert_array_equal(c3["dens_sph"], restatement.sph_density(d2_all))
+
+
+def test_c3_mesh_density(c3, restatement):
+    hb, p, s = c3["hb"], c3["xr"], c3["sample"]
+    mesh, _ = batch.plan_meshes(p.max(0)[None, :], c3["rule"])
+    m = mesh[0]
+    n3 = (int(m["nx"]), int(m["ny"]), int(m["nz"]))
+    assert n3 == (512, 512, 512)
+    o, cell = float(m["xmin"]), float(m["cellsize"])
+    d = restatement.tsc(p[:, 0], p[:, 1], p[:, 2], hb.mass, hb.type, *n3, o, o, o, cell, 5, acc_double=True)
+    S = A.smooth(d.astype(np.float64), A.Mesh.from_desc(m)).ravel()
+    ref = restatement.find_den(p[s, 0], p[s, 1], p[s, 2], S.astype(np.float32), *n3, o, o, o, cell)
+    ref = ref.astype(np.float64)
+    got = c3["dens_mesh"][s].astype(np.float64)
+    hi = ref > 1e-2 * ref.max()
+    assert hi.sum() > 0.05 * len(s)
+    rel = np.abs(got[hi] - ref[hi]) / ref[hi]
+    print(f"mesh density vs FP64 (rho > 1e-2 rho_max): max rel {rel.max():.2e}, median {np.median(rel):.2e}")
+    assert rel.max() < 1e-5
+    # the densest cells collect thousands of TSC contributions, summed in
+    # float (as the reference's deposit): their rounding grows like sqrt(N) u
+    assert np.abs(got - ref).max() < 1e-5 * np.abs(c3["dens_mesh"]).max()
+
+
+def _direct(tpos, sources, targets):
+    """FP64 direct potential (-sum m/r, r > 0) at a few targets."""
+    out = np.zeros(len(targets))
+    sp = sources[:, :3].astype(np.float64)
+    sm = sources[:, 3].astype(np.float64)
+    for t, i in enumerate(targets):
+        for a in range(0, len(sp), 10_000_000):
+            d = sp[a:a + 10_000_000] - tpos[i]
+            r = np.sqrt((d * d).sum(1))
+            ok = r > 0
+            out[t] -= np.sum(sm[a:a + 10_000_000][ok] / r[ok])
+    return out
+
+
+def test_c3_potential_both_opening_angles(c3, restatement):
+    hb, s = c3["hb"], c3["sample"]
+    ph = dropin.physics()
+    p32 = c3["xr"].astype(np.float32)
+    n = hb.n
+    m32 = hb.mass.astype(np.float32)
+    bg = dropin.bg_potent(float(np.sum(m32, dtype=np.float64)))
+    sub = s[:24]
+    direct = _direct(p32.astype(np.float64), c3["tpos"], sub)
+    # theta^2 = 0.5: the stage's own potential against an FP64 walk of its tree
+    phi = restatement.tree_potential(c3["bh"], c3["tpos"], p32[s], np.zeros(len(s), np.int32) + c3["root"][0],
+                                     np.zeros(len(s), np.int32) + c3["rend"][0], None)
+    err = np.abs(c3["penergy"] - (phi * ph["potentfact"] + bg)) / np.abs(phi * ph["potentfact"])
+    assert err.max() < 2e-6, err.max()
+    e05 = np.abs(phi[:24] - direct) / np.abs(direct)
+    # theta = 0.5 (theta^2 = 0.25): the batched potential on its own tree
+    ctx = c3["ctx"]
+    pos4 = np.concatenate([p32, m32[:, None]], 1)
+    _, raw = batch.self_potential(ctx, [0, n], pos4, theta2=0.25, ndirect=100)
+    raw = raw.cpu().numpy()
+    t25 = batch.tree_build_export(ctx, [0, n], pos4, theta2=0.25)
+    phi25 = restatement.tree_potential(t25["bh"], t25["pos"], p32[s], np.zeros(len(s), np.int32) + t25["root"][0],
+                                       np.zeros(len(s), np.int32) + t25["rend"][0], None)
+    assert np.max(np.abs(raw[s] - phi25) / np.abs(phi25)) < 2e-6
+    e025 = np.abs(phi25[:24] - direct) / np.abs(direct)
+    print(f"potential vs FP64 direct (24 targets): theta2=0.5 mean {e05.mean():.2e} max {e05.max():.2e}; "
+          f"theta2=0.25 mean {e025.mean():.2e} max {e025.max():.2e}")
+    assert e025.mean() < e05.mean() < 1e-2
