@@ -214,3 +214,98 @@ def stage_run(ctx: Context, batch: DeviceBatch, cfg: _lib.StageConfig,
     if stats:
         return out, {f: getattr(st, f) for f, _ in _lib.StageStats._fields_}
     return out
+
+
+class PipelinedStage:
+    """The stage over a catalogue split into halo chunks of similar particle
+    counts, each with its own context, CUDA stream, device buffers and host
+    thread, so that one chunk's host<->device copies and host-side syncs
+    (halo frames, tree levels) overlap other chunks' kernels.
+
+    With `prioritise`, earlier chunks get higher stream priorities (CUDA
+    offers four levels through torch), so the GPU works through the chunks
+    roughly in order and fills the gaps of one chunk's host syncs with the
+    next chunk's kernels; the first chunks finish early and their outputs
+    travel back while the later ones compute.
+
+    run_resident() runs every chunk on inputs already on the device;
+    run_e2e() also copies each chunk's inputs from pinned host memory and its
+    outputs back, inside the same overlapped schedule.  Both return the
+    (start, end) CUDA events that bracket all chunks."""
+
+    def __init__(self, hb, cfg: _lib.StageConfig, nchunk: int = 3, device: int = 0, k: int = 32,
+                 prioritise: bool = True):
+        import concurrent.futures as cf
+        self.cfg = cfg
+        self.k = k
+        dev = torch.device("cuda", device)
+        ps = np.asarray(hb.pstart, np.int64)
+        n = int(ps[-1])
+        # halo boundaries closest to equal particle counts
+        cuts = [0]
+        for c in range(1, nchunk):
+            cuts.append(int(np.searchsorted(ps, c * n / nchunk)))
+        cuts.append(len(ps) - 1)
+        cuts = sorted(set(cuts))
+        self.chunks = []
+        _, top = torch.cuda.Stream.priority_range()  # (least, greatest): (0, -3)
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            if b <= a:
+                continue
+            p0, p1 = int(ps[a]), int(ps[b])
+            prio = min(0, top + len(self.chunks)) if prioritise else 0
+            stream = torch.cuda.Stream(device=dev, priority=prio)
+            ctx = Context(device, stream)
+            host = {f: torch.from_numpy(np.ascontiguousarray(getattr(hb, f)[p0:p1], dt)).pin_memory()
+                    for f, dt in (("x", np.float64), ("y", np.float64), ("z", np.float64),
+                                  ("mass", np.float64), ("type", np.int32))}
+            host["pstart"] = torch.from_numpy(ps[a:b + 1] - p0).pin_memory()
+            db = DeviceBatch(*(torch.empty_like(host[f], device=dev) for f in ("x", "y", "z", "mass", "type")),
+                             torch.empty_like(host["pstart"], device=dev))
+            for f in ("x", "y", "z", "mass", "type", "pstart"):
+                getattr(db, f).copy_(host[f])
+            out = StageBuffers(p1 - p0, k, dev)
+            hout = {f: torch.empty(getattr(out, f).shape, dtype=getattr(out, f).dtype).pin_memory()
+                    for f in ("nearindex", "dens_sph", "dens_mesh", "penergy")}
+            self.chunks.append(dict(ctx=ctx, stream=stream, host=host, db=db, out=out, hout=hout, n=p1 - p0))
+        torch.cuda.synchronize(dev)
+        self.pool = cf.ThreadPoolExecutor(max_workers=len(self.chunks))
+        self.h2d_bytes = sum(t.numel() * t.element_size() for c in self.chunks for t in c["host"].values())
+        self.d2h_bytes = sum(t.numel() * t.element_size() for c in self.chunks for t in c["hout"].values())
+
+    def _chunk(self, c, e2e: bool, start):
+        s = c["stream"]
+        s.wait_event(start)
+        if e2e:
+            with torch.cuda.stream(s):
+                for f in ("x", "y", "z", "mass", "type", "pstart"):
+                    getattr(c["db"], f).copy_(c["host"][f], non_blocking=True)
+        stage_run(c["ctx"], c["db"], self.cfg, c["out"])
+        if e2e:
+            with torch.cuda.stream(s):
+                for f, t in c["hout"].items():
+                    t.copy_(getattr(c["out"], f), non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(s)
+        return done
+
+    def _run(self, e2e: bool):
+        cur = torch.cuda.current_stream()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(cur)
+        dones = list(self.pool.map(lambda c: self._chunk(c, e2e, start), self.chunks))
+        for d in dones:
+            cur.wait_event(d)
+        end.record(cur)
+        return start, end
+
+    def run_resident(self):
+        return self._run(False)
+
+    def run_e2e(self):
+        return self._run(True)
+
+    def close(self):
+        self.pool.shutdown()
+        for c in self.chunks:
+            c["ctx"].close()
