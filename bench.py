@@ -421,6 +421,22 @@ def main():
                     "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": None,
                     "peak_source": pk["source"], "dominant_phase": dom}
 
+    # the kNN kernel's own work counters, per query
+    if _lib.tuning_value("GF_KNN_ALGO") == 1:
+        names = ("node_tests_per_bucket", "particle_tests_per_bucket", "heap_insertions",
+                 "warp_insertion_steps_per_bucket", "buckets_per_query")
+        per = {"node_tests_per_bucket": 32, "particle_tests_per_bucket": 32,
+               "warp_insertion_steps_per_bucket": 32}
+        kernel = "knn_bucket_kernel (lane = query, 32 tree-order queries per warp)"
+    else:
+        names = ("nodes", "batches", "candidates", "single_inserts", "bitonic_merges")
+        per = {}
+        kernel = "knn_kernel (warp = query)"
+    knn_work = {"kernel": kernel}
+    for nm, key in zip(names, ("knn_nodes", "knn_batches", "knn_candidates", "knn_single_inserts",
+                               "knn_bitonic_merges")):
+        knn_work[nm] = st[key] / max(hb.n, 1) * per.get(nm, 1)
+
     line = dict(base)
     line.update({
         "value": pipe_res["resident"]["value"], "ms_per_step": pipe_res["resident"]["ms_per_step"],
@@ -443,9 +459,7 @@ def main():
         "phases_ms": phases,
         "interactions": {"particle_particle": st["pp_interactions"],
                          "particle_cell": st["pc_interactions"]},
-        "knn_work_per_query": {k[4:]: st[k] / max(hb.n, 1) for k in
-                               ("knn_nodes", "knn_batches", "knn_candidates",
-                                "knn_single_inserts", "knn_bitonic_merges")},
+        "knn_work_per_query": knn_work,
         "plain": plain,
         "gpu_launches": int(pipe_res["resident"]["launches"]),
         "clocks": clk,

@@ -150,6 +150,7 @@ SIGNATURES = {
     "gf_last_error": (ctypes.c_char_p, []),
     "gf_set_device": (_INT, [_INT]),
     "gf_kernel_launch_count": (ctypes.c_uint64, []),
+    "gf_tuning_value": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
     "gf_set_cosmology": (_INT, [_F, _F, _F, _F, _F]),
     "gf_get_physics": (_INT, [ctypes.POINTER(Physics)]),
     "gf_bg_potent": (_D, [_D]),
@@ -229,6 +230,13 @@ def ptr(a) -> int:
     if isinstance(a, np.ndarray):
         return a.ctypes.data
     return a.data_ptr()
+
+
+def tuning_value(name: str) -> int:
+    """A compile-time launch parameter of the loaded libgf (gf_tuning.cuh)."""
+    v = ctypes.c_int64()
+    check(lib().gf_tuning_value(name.encode(), ctypes.byref(v)))
+    return int(v.value)
 
 
 def exported_symbols() -> list[str]:

@@ -297,6 +297,26 @@ int gf_set_device(int device) {
 
 uint64_t gf_kernel_launch_count(void) { return g_launches.load(); }
 
+int gf_tuning_value(const char *name, int64_t *value) {
+    clear_status();
+    static const struct {
+        const char *name;
+        int64_t value;
+    } params[] = {{"GF_KNN_ALGO", GF_KNN_ALGO},       {"GF_KNNB_BLOCK", GF_KNNB_BLOCK},
+                  {"GF_KNNB_ARITY", GF_KNNB_ARITY},   {"GF_KNN_BLOCK", GF_KNN_BLOCK},
+                  {"GF_KNN_MINB", GF_KNN_MINB},       {"GF_KNN_CHUNK", GF_KNN_CHUNK},
+                  {"GF_BH_BLOCK", GF_BH_BLOCK},       {"GF_BH_MINB", GF_BH_MINB},
+                  {"GF_FFT_PENCILS", GF_FFT_PENCILS}, {"GF_TREE_BLOCK", GF_TREE_BLOCK}};
+    if (!name || !value) return GF_EINVAL;
+    for (const auto &p : params)
+        if (strcmp(p.name, name) == 0) {
+            *value = p.value;
+            return GF_OK;
+        }
+    set_status(GF_EINVAL, "unknown tuning parameter %s", name);
+    return GF_EINVAL;
+}
+
 int gf_set_cosmology(float amax, float a, float omep, float omeplam, float hubble) {
     ensure_physics();
     g_phys.amax = amax;

@@ -2,8 +2,11 @@
 //
 // The reference (NewGalFinder/nnost.c:375-422 Find_Near, :560-630
 // findsphdensity) walks a COM octree per particle and keeps a sorted list of
-// the k closest particles, self included.  Here one warp serves one query at
-// a time, walking a chunk of consecutive tree-order queries:
+// the k closest particles, self included.  Two kernels compute the same
+// lists (GF_KNN_ALGO selects; the autotuner keeps the faster):
+// knn_bucket_kernel (below) walks once per 32 tree-order queries with one
+// query per lane; knn_kernel serves one query per warp, walking a chunk of
+// consecutive tree-order queries:
 //   * the sorted list (k <= 32) lives in registers, entry j in lane j;
 //   * the list starts as the k closest of the previous query's list (or,
 //     for the first query of a chunk, of the 32 tree-order neighbours), with
@@ -420,6 +423,305 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
         for (int i = 0; i < 5; i++) atomicAdd(counters + i, ctr[i]);
 }
 
+// ---------------------------------------------------------------- bucket kNN
+// One warp serves a bucket of 32 consecutive tree-order queries, one per
+// lane, and walks the tree once for all of them: a node is entered when its
+// box lies within the bound of any lane, and each of its loose particles is
+// tested by every lane against its own query.  Neighbouring queries share
+// most of their candidates, so the walk, the node tests and the particle
+// loads are paid once per bucket rather than once per query.  Each lane keeps
+// its k closest as a max-heap (GF_KNNB_ARITY children per node) keyed by
+// (exact FP64 distance^2, batch index) in its own column of a per-warp
+// shared-memory array (column = lane: every access is conflict-free however
+// the lanes' heap positions diverge).
+//   * Seeds: every lane's heap starts as its query's min(32, halo size)
+//     tree-order neighbours (heapified), which bounds its k-th distance before
+//     the walk; the walk skips them.
+//   * Walk: bottom-up as in knn_kernel, starting at the smallest subtree that
+//     holds the whole bucket, then each ancestor's range minus the subtree
+//     already walked, until every lane's ball lies inside the processed box.
+//   * Output: an in-place heapsort gives the ascending list; the density is
+//     summed in list order as in knn_kernel.
+// The prefilters and the exact keys are those of knn_kernel, so the lists
+// and densities are bit-identical.
+constexpr int kHeapBytes = 32 * 32 * (int)(sizeof(double) + sizeof(int));
+constexpr int kBucketWarpBytes = kHeapBytes + 32 * (int)sizeof(KnnNode) + 32 * 16 + 32 * 4;
+static_assert(sizeof(KnnNode) == 48, "KnnNode is copied as 12 words");
+
+// f_d2 with fused multiply-adds: at most four roundings after the exact-input
+// differences, so the relative error stays below the 6u that kSlack covers.
+__device__ __forceinline__ float f_d2_fma(const float4 &a, const float4 &b) {
+    const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    return __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+}
+
+struct LaneHeap {
+    double *D;  // this lane's column: entry e at D[32 * e]
+    int *I;
+    int kk;
+    double bd;  // root key: the bound
+    int bi;
+    float bf;   // float prefilter bound: (float)bd * (1 + kSlack)
+};
+
+constexpr int kArity = GF_KNNB_ARITY;  // children per heap node
+
+// Places (kd, ki) at the hole `pos` and moves it down to restore the max-heap
+// over entries [0, size).
+__device__ __forceinline__ void heap_sift_down(double *D, int *I, int pos, int size, double kd, int ki) {
+    while (true) {
+        const int c0 = kArity * pos + 1;
+        if (c0 >= size) break;
+        int c = c0;
+        double cd = D[32 * c0];
+        int ci = I[32 * c0];
+#pragma unroll
+        for (int u = 1; u < kArity; u++) {
+            if (c0 + u < size) {
+                const double rd = D[32 * (c0 + u)];
+                const int ri = I[32 * (c0 + u)];
+                if (key_lt(cd, ci, rd, ri)) {
+                    c = c0 + u;
+                    cd = rd;
+                    ci = ri;
+                }
+            }
+        }
+        if (!key_lt(kd, ki, cd, ci)) break;
+        D[32 * pos] = cd;
+        I[32 * pos] = ci;
+        pos = c;
+    }
+    D[32 * pos] = kd;
+    I[32 * pos] = ki;
+}
+
+__device__ __forceinline__ void heap_set_bound(LaneHeap &H) {
+    H.bd = H.D[0];
+    H.bi = H.I[0];
+    H.bf = (float)H.bd * (1.f + kSlack);
+}
+
+// Replaces the root (the largest key) by (kd, ki), which is below it.
+__device__ __forceinline__ void heap_put(LaneHeap &H, double kd, int ki) {
+    heap_sift_down(H.D, H.I, 0, H.kk, kd, ki);
+    heap_set_bound(H);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(GF_KNNB_BLOCK, GF_KNNB_MINB)
+knn_bucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__restrict__ perm,
+                  const int32_t *__restrict__ phalo, const int64_t *__restrict__ pstart,
+                  const int32_t *__restrict__ owner, const KnnNode *__restrict__ nodes,
+                  int32_t *__restrict__ nearindex, float *__restrict__ dens, int *err,
+                  unsigned long long *__restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * kBucketWarpBytes;
+    double *HD = reinterpret_cast<double *>(ws);
+    int *HI = reinterpret_cast<int *>(ws + 32 * 32 * sizeof(double));
+    KnnNode *win = reinterpret_cast<KnnNode *>(ws + kHeapBytes);
+    float4 *cpos = reinterpret_cast<float4 *>(ws + kHeapBytes + 32 * sizeof(KnnNode));
+    int *cid = reinterpret_cast<int *>(cpos + 32);
+    int *win_w = reinterpret_cast<int *>(win);
+    const int *nodes_w = reinterpret_cast<const int *>(nodes);
+    // work counters: node tests, 32-wide particle loads, heap insertions
+    // (per lane), warp-wide insertion steps, buckets
+    unsigned long long ctr[5] = {0, 0, 0, 0, 0};
+    const bool vec_out = k % 4 == 0 && ((uintptr_t)nearindex & 15) == 0;
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nbucket = (n + 31) >> 5;
+    for (int64_t bucket = wid; bucket < nbucket; bucket += nwarps) {
+        const int64_t b = bucket << 5;
+        const int64_t q = b + lane;
+        const bool valid = q < n;
+        const int h = valid ? phalo[q] : -1;
+        const float4 Q = valid ? pos[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const double Qx = Q.x, Qy = Q.y, Qz = Q.z;
+        const int myid = valid ? perm[q] : INT_MAX;
+        unsigned remaining = __ballot_sync(0xffffffffu, valid);
+        // one pass per halo present in the bucket (its lanes are contiguous)
+        while (remaining) {
+            const int leader = __ffs(remaining) - 1;
+            const int hl = __shfl_sync(0xffffffffu, h, leader);
+            const unsigned act = __ballot_sync(0xffffffffu, valid && h == hl);
+            remaining &= ~act;
+            const bool me = (act >> lane) & 1;
+            const int qa = (int)(b + leader);
+            const int qb = (int)(b + 31 - __clz(act));
+            const int64_t hs = pstart[hl];
+            const int64_t he = pstart[hl + 1];
+            const int kk = (int)min((int64_t)k, he - hs);
+            LaneHeap H;
+            H.D = HD + lane;
+            H.I = HI + lane;
+            H.kk = kk;
+            // ---- seeds: the min(32, halo size) tree-order neighbours of the
+            // lane's query (>= kk particles, so the heap is full and bounds
+            // the walk from its first node); the walk skips them
+            const int ns = (int)min((int64_t)32, he - hs);
+            int64_t sw = q - 16;
+            if (sw + ns > he) sw = he - ns;
+            if (sw < hs) sw = hs;
+            const int sw0 = (int)sw, sw1 = (int)sw + ns;
+            if (me) {
+                for (int t = 0; t < kk; t++) {
+                    H.D[32 * t] = exact_d2(Q, pos[sw0 + t]);
+                    H.I[32 * t] = perm[sw0 + t];
+                }
+                for (int e = (kk - 2) / kArity; e >= 0; e--) heap_sift_down(H.D, H.I, e, kk, H.D[32 * e], H.I[32 * e]);
+                heap_set_bound(H);
+                for (int t = kk; t < ns; t++) {
+                    const double d = exact_d2(Q, pos[sw0 + t]);
+                    const int sid = perm[sw0 + t];
+                    if (key_lt(d, sid, H.bd, H.bi)) heap_put(H, d, sid);
+                }
+            } else {
+                H.bd = kInf;
+                H.bi = INT_MAX;
+                H.bf = 0.f;
+            }
+            // ---- the smallest subtree holding [qa, qb]
+            int c = owner[qa];
+            KnnNode C = nodes[c];
+            while (!(C.lstart <= qa && qb < C.lstart + C.count) && C.parent >= 0) {
+                c = C.parent;
+                C = nodes[c];
+            }
+            int w0 = c, w1 = C.skip, x0 = -1, x1 = -1;
+            while (true) {
+                // ---- stackless preorder walk of [w0, w1) minus [x0, x1)
+                int i = w0, wb = INT_MIN / 2;
+                while (i < w1) {
+                    if (i == x0) {
+                        i = x1;
+                        continue;
+                    }
+                    if (i >= wb + 32 || i < wb) {  // window of 32 nodes at i
+                        wb = i;
+                        const int nw = min(32, w1 - wb) * 12;
+                        __syncwarp();
+                        for (int t = lane; t < nw; t += 32) win_w[t] = nodes_w[(int64_t)wb * 12 + t];
+                        __syncwarp();
+                    }
+                    const float4 *nv = reinterpret_cast<const float4 *>(win + (i - wb));
+                    const float4 n0 = nv[0], n1 = nv[1];
+                    const float gx = fmaxf(fmaxf(n0.x - Q.x, Q.x - n0.w), 0.f);
+                    const float gy = fmaxf(fmaxf(n0.y - Q.y, Q.y - n1.x), 0.f);
+                    const float gz = fmaxf(fmaxf(n0.z - Q.z, Q.z - n1.y), 0.f);
+                    const float lb = gx * gx + gy * gy + gz * gz;
+                    if (COUNT) ctr[0]++;
+                    if (!__any_sync(0xffffffffu, me && lb <= H.bf)) {
+                        i = __float_as_int(n1.z);  // skip
+                        continue;
+                    }
+                    const int l0 = __float_as_int(n1.w);
+                    const int l1 = l0 + __float_as_int(nv[2].x);
+                    for (int base = l0; base < l1; base += 32) {
+                        const int j = base + lane;
+                        __syncwarp();
+                        if (j < l1) {
+                            cpos[lane] = pos[j];
+                            cid[lane] = perm[j];
+                        }
+                        __syncwarp();
+                        const int m = min(32, l1 - base);
+                        if (COUNT) ctr[1] += m;
+                        // four candidates in flight: their float distances are
+                        // independent; the bound is re-read after each insertion
+                        for (int t0 = 0; t0 < m; t0 += 4) {
+                            float4 S[4];
+                            float f[4];
+#pragma unroll
+                            for (int u = 0; u < 4; u++) {
+                                S[u] = cpos[t0 + u];  // t0 + u <= 31; entries >= m are ignored
+                                f[u] = f_d2_fma(Q, S[u]);
+                            }
+#pragma unroll
+                            for (int u = 0; u < 4; u++) {
+                                const int p = base + t0 + u;
+                                bool ins = false;
+                                if (me && t0 + u < m && f[u] <= H.bf && (p < sw0 || p >= sw1)) {
+                                    const double dx = Qx - (double)S[u].x;
+                                    const double dy = Qy - (double)S[u].y;
+                                    const double dz = Qz - (double)S[u].z;
+                                    const double d = dx * dx + dy * dy + dz * dz;
+                                    const int sid = cid[t0 + u];
+                                    if (key_lt(d, sid, H.bd, H.bi)) {
+                                        heap_put(H, d, sid);
+                                        ins = true;
+                                    }
+                                }
+                                if (COUNT) {
+                                    ctr[2] += ins;
+                                    ctr[3] += __any_sync(0xffffffffu, ins);
+                                }
+                            }
+                        }
+                    }
+                    i++;
+                }
+                const bool done = !me || ball_inside(Q, H.bd, C);
+                if (C.parent < 0 || __all_sync(0xffffffffu, done)) break;
+                const int a = C.parent;
+                const KnnNode A = nodes[a];
+                w0 = a;
+                w1 = A.skip;
+                x0 = c;
+                x1 = C.skip;
+                c = a;
+                C = A;
+            }
+            if (COUNT) ctr[4]++;
+            // ---- outputs in batch order
+            if (me) {
+                {  // heapsort: ascending keys
+                    for (int e = kk - 1; e > 0; e--) {
+                        const double td = H.D[32 * e];
+                        const int ti = H.I[32 * e];
+                        H.D[32 * e] = H.D[0];
+                        H.I[32 * e] = H.I[0];
+                        heap_sift_down(H.D, H.I, 0, e, td, ti);
+                    }
+                    int32_t *row = nearindex + (int64_t)myid * k;
+                    if (vec_out) {
+                        for (int j = 0; j < k; j += 4) {
+                            int4 v;
+                            v.x = j < kk ? (int32_t)(H.I[32 * j] - hs) : -1;
+                            v.y = j + 1 < kk ? (int32_t)(H.I[32 * (j + 1)] - hs) : -1;
+                            v.z = j + 2 < kk ? (int32_t)(H.I[32 * (j + 2)] - hs) : -1;
+                            v.w = j + 3 < kk ? (int32_t)(H.I[32 * (j + 3)] - hs) : -1;
+                            *reinterpret_cast<int4 *>(row + j) = v;
+                        }
+                    } else {
+                        for (int j = 0; j < k; j++) row[j] = j < kk ? (int32_t)(H.I[32 * j] - hs) : -1;
+                    }
+                    if (dens) {
+                        // nnost.c:292,415: maxr = sqrtf(maxdist2); W4(sqrtf(d2_j), maxr/2.)
+                        const float neardist = sqrtf((float)H.D[32 * (kk - 1)]);
+                        const float hh = (float)(neardist / 2.);
+                        float rho = 0.f;
+                        for (int j = 0; j < kk; j++) rho += w4(sqrtf((float)H.D[32 * j]), hh);
+                        dens[myid] = rho;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (COUNT && counters) {
+        for (int off = 16; off; off >>= 1) ctr[2] += __shfl_xor_sync(0xffffffffu, ctr[2], off);
+        if (lane == 0) {
+            atomicAdd(counters + 0, ctr[0]);
+            atomicAdd(counters + 1, ctr[1]);
+            atomicAdd(counters + 2, ctr[2]);
+            atomicAdd(counters + 3, ctr[3]);
+            atomicAdd(counters + 4, ctr[4]);
+        }
+    }
+}
+
 }  // namespace
 
 int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const float4 *pos_batch, int k,
@@ -431,6 +733,21 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
     }
     const int64_t nquery = qlist ? nq : t.n;
     if (t.n <= 0 || nquery <= 0) return GF_OK;
+    if (GF_KNN_ALGO == 1 && !qlist) {
+        const int block = GF_KNNB_BLOCK;
+        const size_t shmem = (size_t)(block / 32) * kBucketWarpBytes;
+        int per_sm = 0;
+        auto kern = counters ? knn_bucket_kernel<true> : knn_bucket_kernel<false>;
+        GF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+        GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, shmem));
+        const int64_t nbucket = (t.n + 31) / 32;
+        int64_t grid = (nbucket * 32 + block - 1) / block;
+        grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * std::max(per_sm, 1)));
+        kern<<<(int)grid, block, shmem, ctx->stream>>>(t.n, k, t.pos, t.perm, t.phalo, pstart, t.owner, t.knn,
+                                                       nearindex, dens, ctx->d_err, counters);
+        GF_LAUNCH_CHECK();
+        return GF_OK;
+    }
     const int block = GF_KNN_BLOCK;
     const int64_t warps_needed = (nquery + kChunk - 1) / kChunk;
     int64_t grid = (warps_needed * 32 + block - 1) / block;

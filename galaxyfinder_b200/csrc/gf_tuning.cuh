@@ -13,6 +13,18 @@
 #ifndef GF_KNN_CHUNK   // consecutive tree-order queries per warp task
 #define GF_KNN_CHUNK 32
 #endif
+#ifndef GF_KNN_ALGO    // 1: bucket kNN (a warp walks once for 32 tree-order queries,
+#define GF_KNN_ALGO 1  //    lane = query); 0: one warp per query
+#endif
+#ifndef GF_KNNB_BLOCK  // threads per block of knn_bucket_kernel (14.5 KB shared memory per warp)
+#define GF_KNNB_BLOCK 32
+#endif
+#ifndef GF_KNNB_MINB
+#define GF_KNNB_MINB 1
+#endif
+#ifndef GF_KNNB_ARITY  // children per node of the bucket kernel's per-lane heaps (2 or 4)
+#define GF_KNNB_ARITY 2
+#endif
 #ifndef GF_BH_BLOCK    // threads per block of bh_kernel
 #define GF_BH_BLOCK 128
 #endif
@@ -28,6 +40,9 @@
 
 static_assert(GF_KNN_BLOCK % 32 == 0 && GF_KNN_BLOCK <= 1024, "GF_KNN_BLOCK");
 static_assert(GF_KNN_CHUNK >= 1, "GF_KNN_CHUNK");
+static_assert(GF_KNNB_BLOCK % 32 == 0 && GF_KNNB_BLOCK <= 512, "GF_KNNB_BLOCK");
+static_assert(GF_KNN_ALGO == 0 || GF_KNN_ALGO == 1, "GF_KNN_ALGO");
+static_assert(GF_KNNB_ARITY == 2 || GF_KNNB_ARITY == 4, "GF_KNNB_ARITY");
 static_assert(GF_BH_BLOCK % 32 == 0 && GF_BH_BLOCK <= 1024, "GF_BH_BLOCK");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");
 static_assert(GF_TREE_BLOCK % 32 == 0 && GF_TREE_BLOCK >= 128 && GF_TREE_BLOCK <= 1024, "GF_TREE_BLOCK");

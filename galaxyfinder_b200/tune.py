@@ -11,7 +11,8 @@ result goes to galaxyfinder_b200/tuned.json (parameters, every measurement,
 the GPU and the workload), which build.py turns into -D flags.
 
   group   parameters                                   phase
-  knn     GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
+  knn     GF_KNN_ALGO x GF_KNNB_BLOCK x GF_KNNB_ARITY; for the warp-per-query
+          kernel GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
   bh      GF_BH_BLOCK, then the register cap           potential
   fft     GF_FFT_PENCILS                               smooth
   tree    GF_TREE_BLOCK                                tree
@@ -34,7 +35,8 @@ from pathlib import Path
 from . import build as B
 
 TUNE_DIR = B.PKG / "_tune"
-DEFAULTS = {"GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32, "GF_BH_BLOCK": 128,
+DEFAULTS = {"GF_KNN_ALGO": 1, "GF_KNNB_BLOCK": 32, "GF_KNNB_ARITY": 2, "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
+            "GF_BH_BLOCK": 128,
             "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
 
@@ -43,18 +45,22 @@ def minb(block: int, regs: int) -> int:
     return max(1, 65536 // (block * regs)) if regs < 255 else 1
 
 
-# group -> (source file, phase, list of stages; each stage = list of overrides)
-def stages(group: str, base: dict) -> list[list[dict]]:
+# group -> stages; each stage maps the current best parameters to a list of
+# overrides (an empty list skips the stage)
+def stages(group: str):
     if group == "knn":
-        return [[{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
+        return [lambda base: [{"GF_KNN_ALGO": 1, "GF_KNNB_BLOCK": b, "GF_KNNB_ARITY": a}
+                              for b in (32, 64) for a in (2, 4)] + [{"GF_KNN_ALGO": 0}],
+                lambda base: [] if base["GF_KNN_ALGO"] == 1 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
+                lambda base: [] if base["GF_KNN_ALGO"] == 1 else
                 [{"GF_KNN_BLOCK": b, "GF_KNN_MINB": minb(b, r)} for b in (128, 256) for r in REGCAPS]]
     if group == "bh":
-        return [[{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],
-                [{"GF_BH_MINB": minb(base["GF_BH_BLOCK"], r)} for r in REGCAPS]]
+        return [lambda base: [{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],
+                lambda base: [{"GF_BH_MINB": minb(base["GF_BH_BLOCK"], r)} for r in REGCAPS]]
     if group == "fft":
-        return [[{"GF_FFT_PENCILS": p} for p in (16, 32)]]
+        return [lambda base: [{"GF_FFT_PENCILS": p} for p in (16, 32)]]
     if group == "tree":
-        return [[{"GF_TREE_BLOCK": b} for b in (128, 256, 512)]]
+        return [lambda base: [{"GF_TREE_BLOCK": b} for b in (128, 256, 512)]]
     raise ValueError(group)
 
 
@@ -119,7 +125,10 @@ def tune(nhalo: int, steps: int, groups=("knn", "bh", "fft", "tree")) -> dict:
     for g in groups:
         src, phase = GROUPS[g]
         log[g] = []
-        for stage in stages(g, base):
+        for stage_fn in stages(g):
+            stage = stage_fn(base)
+            if not stage:
+                continue
             cands = [dict(base, **ov) for ov in stage]
             with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
                 libs = list(ex.map(lambda p: build_variant(src, p), cands))
@@ -136,6 +145,10 @@ def tune(nhalo: int, steps: int, groups=("knn", "bh", "fft", "tree")) -> dict:
             if ref_ms is None or ms < 0.99 * ref_ms:  # keep the incumbent unless >1% faster
                 base = p
     import torch
+    if B.TUNED.exists():  # keep the measurements of the groups not re-run
+        prev = json.loads(B.TUNED.read_text())
+        log = {**prev.get("measured", {}), **log}
+        groups = tuple(dict.fromkeys(list(prev.get("phase_of_group", {})) + list(groups)))
     res = {"params": base, "measured": log, "phase_of_group": {g: GROUPS[g][1] for g in groups},
            "workload": f"seeded catalogue, {nhalo} halos (N_p ~ N^-1.9 on [100, 2e6]), best of {steps} steps",
            "gpu": torch.cuda.get_device_name(0), "date": datetime.date.today().isoformat()}

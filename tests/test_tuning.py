@@ -7,6 +7,8 @@ from galaxyfinder_b200 import tune as T
 
 
 def _valid(p):
+    assert p["GF_KNN_ALGO"] in (0, 1)
+    assert p["GF_KNNB_BLOCK"] % 32 == 0 and p["GF_KNNB_BLOCK"] <= 512
     assert p["GF_KNN_BLOCK"] % 32 == 0 and p["GF_KNN_BLOCK"] <= 1024
     assert p["GF_BH_BLOCK"] % 32 == 0 and p["GF_BH_BLOCK"] <= 1024
     assert p["GF_FFT_PENCILS"] % 2 == 0 and (p["GF_FFT_PENCILS"] // 2) * 512 // 8 <= 1024
@@ -16,12 +18,18 @@ def _valid(p):
 
 
 def test_search_space_is_valid():
-    base = dict(T.DEFAULTS)
-    for g in T.GROUPS:
-        for stage in T.stages(g, base):
-            assert stage
-            for ov in stage:
-                _valid(dict(base, **ov))
+    # both kNN kernels: the warp-per-query stages open up when it wins
+    for algo in (0, 1):
+        base = dict(T.DEFAULTS, GF_KNN_ALGO=algo)
+        for g in T.GROUPS:
+            nonempty = 0
+            for stage_fn in T.stages(g):
+                stage = stage_fn(base)
+                nonempty += bool(stage)
+                for ov in stage:
+                    _valid(dict(base, **ov))
+            assert nonempty >= 1
+        assert len(T.stages("knn")[1](base)) == (3 if algo == 0 else 0)
 
 
 def test_tuned_params_become_flags(tmp_path, monkeypatch):
