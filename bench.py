@@ -422,12 +422,16 @@ def main():
                     "peak_source": pk["source"], "dominant_phase": dom}
 
     # the kNN kernel's own work counters, per query
-    if _lib.tuning_value("GF_KNN_ALGO") == 1:
+    algo = _lib.tuning_value("GF_KNN_ALGO")
+    if algo in (1, 2):
         names = ("node_tests_per_bucket", "particle_tests_per_bucket", "heap_insertions",
-                 "warp_insertion_steps_per_bucket", "buckets_per_query")
+                 "warp_insertion_steps_per_bucket",
+                 "buckets_per_query" if algo == 1 else "uncertified_fraction")
         per = {"node_tests_per_bucket": 32, "particle_tests_per_bucket": 32,
                "warp_insertion_steps_per_bucket": 32}
-        kernel = "knn_bucket_kernel (lane = query, 32 tree-order queries per warp)"
+        kernel = ("knn_bucket_kernel (lane = query, 32 tree-order queries per warp)" if algo == 1 else
+                  "knn_fbucket_kernel (lane = query, float heap keys, exact FP64 certification; "
+                  "uncertified queries redone by knn_kernel)")
     else:
         names = ("nodes", "batches", "candidates", "single_inserts", "bitonic_merges")
         per = {}

@@ -2,11 +2,12 @@
 //
 // The reference (NewGalFinder/nnost.c:375-422 Find_Near, :560-630
 // findsphdensity) walks a COM octree per particle and keeps a sorted list of
-// the k closest particles, self included.  Two kernels compute the same
-// lists (GF_KNN_ALGO selects; the autotuner keeps the faster):
-// knn_bucket_kernel (below) walks once per 32 tree-order queries with one
-// query per lane; knn_kernel serves one query per warp, walking a chunk of
-// consecutive tree-order queries:
+// the k closest particles, self included.  Three kernels compute the same
+// lists (GF_KNN_ALGO selects; the autotuner keeps the fastest):
+// knn_bucket_kernel and knn_fbucket_kernel (below) walk once per 32
+// tree-order queries with one query per lane (the second with float keys and
+// an exact certification); knn_kernel serves one query per warp, walking a
+// chunk of consecutive tree-order queries:
 //   * the sorted list (k <= 32) lives in registers, entry j in lane j;
 //   * the list starts as the k closest of the previous query's list (or,
 //     for the first query of a chunk, of the 32 tree-order neighbours), with
@@ -313,7 +314,12 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
            const int64_t *__restrict__ pstart, const int32_t *__restrict__ owner,
            const KnnNode *__restrict__ nodes, int32_t *__restrict__ nearindex,
            float *__restrict__ dens, int *err, unsigned long long *__restrict__ counters,
-           const int32_t *__restrict__ qlist) {
+           const int32_t *__restrict__ qlist, const unsigned *__restrict__ nq_dev = nullptr,
+           bool natural_rows = false) {
+    // nq_dev: the query count lives in device memory (qlist filled by an
+    // earlier kernel); natural_rows: outputs go to the query's batch row
+    // perm[q] rather than to row qi of the list
+    if (nq_dev) n = *nq_dev;
     const int lane = threadIdx.x & 31;
     __shared__ int seeded_set[GF_KNN_BLOCK / 32][kSetSlots];
     int *seeded = seeded_set[threadIdx.x >> 5];
@@ -408,7 +414,7 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
                 continue;
             }
             // ---- outputs in batch order
-            const int64_t qo = qlist ? qi : (int64_t)perm[q];
+            const int64_t qo = qlist && !natural_rows ? qi : (int64_t)perm[q];
             if (lane < k) nearindex[(int64_t)qo * k + lane] = lane < kk ? (int32_t)(L.Li - hs) : -1;
             // nnost.c:292,415: maxr = sqrtf(maxdist2); W4(sqrtf(d2_j), maxr/2.)
             const float neardist = sqrtf((float)__shfl_sync(0xffffffffu, L.Ld, kk - 1));
@@ -722,6 +728,276 @@ knn_bucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_
     }
 }
 
+// ------------------------------------------------- bucket kNN, float keys
+// As knn_bucket_kernel, but each lane's heap holds packed 64-bit keys
+// (float distance^2 bits << 32 | batch index): non-negative float bit
+// patterns order like the floats, so one integer compare orders (f, index).
+// The walk needs no FP64 and the heaps take 8 KB per warp instead of 12 KB
+// (more resident warps).  Float keys can misorder particles whose exact
+// distances agree to ~6u, so the result is certified per query: every
+// particle not kept has a float distance (or lies in a node whose float box
+// distance was) at least frej, or lies outside the box of the processed
+// subtree (exact distance >= the box distance dbox), and floats are within
+// 6u of the exact value; the kept k are re-ranked by their exact FP64
+// distances, and the list is exact when the largest kept exact distance is
+// below min(frej (1 - 2e-6), dbox^2).  A query that fails (near-ties at the
+// k-th place, duplicate positions) goes to a device list that knn_kernel
+// then serves exactly.  Output rows and densities are written by the warp one
+// query at a time (coalesced), in the arithmetic of knn_kernel.
+constexpr int kFBucketWarpBytes = 32 * 32 * 8 + 32 * (int)sizeof(KnnNode) + 32 * 16 + 32 * 4;
+
+__device__ __forceinline__ uint64_t pack_key(float f, int id) {
+    return ((uint64_t)__float_as_uint(f) << 32) | (uint32_t)id;
+}
+__device__ __forceinline__ float key_f(uint64_t key) { return __uint_as_float((unsigned)(key >> 32)); }
+
+// Max-heap of packed keys in one lane's column (entry e at K[32 e]).
+__device__ __forceinline__ void kheap_sift_down(uint64_t *K, int pos, int size, uint64_t key) {
+    while (true) {
+        int c = 2 * pos + 1;
+        if (c >= size) break;
+        uint64_t ck = K[32 * c];
+        if (c + 1 < size) {
+            const uint64_t rk = K[32 * (c + 1)];
+            if (rk > ck) {
+                c++;
+                ck = rk;
+            }
+        }
+        if (key > ck) break;
+        K[32 * pos] = ck;
+        pos = c;
+    }
+    K[32 * pos] = key;
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(GF_KNNB_BLOCK, GF_KNNB_MINB)
+knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__restrict__ perm,
+                   const float4 *__restrict__ pos_batch, const int32_t *__restrict__ phalo,
+                   const int64_t *__restrict__ pstart, const int32_t *__restrict__ owner,
+                   const KnnNode *__restrict__ nodes, int32_t *__restrict__ nearindex,
+                   float *__restrict__ dens, int32_t *__restrict__ redo, unsigned *__restrict__ nredo,
+                   unsigned long long *__restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * kFBucketWarpBytes;
+    uint64_t *KH = reinterpret_cast<uint64_t *>(ws);
+    KnnNode *win = reinterpret_cast<KnnNode *>(ws + 32 * 32 * 8);
+    float4 *cpos = reinterpret_cast<float4 *>(ws + 32 * 32 * 8 + 32 * sizeof(KnnNode));
+    int *cid = reinterpret_cast<int *>(cpos + 32);
+    int *win_w = reinterpret_cast<int *>(win);
+    const int *nodes_w = reinterpret_cast<const int *>(nodes);
+    uint64_t *K = KH + lane;  // this lane's heap column
+    // work counters: node tests, particle tests, heap insertions (per lane),
+    // warp-wide insertion steps, queries sent to the exact kernel
+    unsigned long long ctr[5] = {0, 0, 0, 0, 0};
+    const float kInfF = __int_as_float(0x7f800000);
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nbucket = (n + 31) >> 5;
+    for (int64_t bucket = wid; bucket < nbucket; bucket += nwarps) {
+        const int64_t b = bucket << 5;
+        const int64_t q = b + lane;
+        const bool valid = q < n;
+        const int h = valid ? phalo[q] : -1;
+        const float4 Q = valid ? pos[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int myid = valid ? perm[q] : INT_MAX;
+        unsigned remaining = __ballot_sync(0xffffffffu, valid);
+        while (remaining) {
+            const int leader = __ffs(remaining) - 1;
+            const int hl = __shfl_sync(0xffffffffu, h, leader);
+            const unsigned act = __ballot_sync(0xffffffffu, valid && h == hl);
+            remaining &= ~act;
+            const bool me = (act >> lane) & 1;
+            const int qa = (int)(b + leader);
+            const int qb = (int)(b + 31 - __clz(act));
+            const int64_t hs = pstart[hl];
+            const int64_t he = pstart[hl + 1];
+            const int kk = (int)min((int64_t)k, he - hs);
+            // ---- seeds: the query's min(32, halo size) tree-order neighbours
+            const int ns = (int)min((int64_t)32, he - hs);
+            int64_t sw = q - 16;
+            if (sw + ns > he) sw = he - ns;
+            if (sw < hs) sw = hs;
+            const int sw0 = (int)sw, sw1 = (int)sw + ns;
+            uint64_t rk = ~0ull;  // root key (the bound)
+            float bf = 0.f;       // its float distance
+            float frej = kInfF;   // least float distance (or box bound) of everything not kept
+            if (me) {
+                for (int t = 0; t < kk; t++) K[32 * t] = pack_key(f_d2_fma(Q, pos[sw0 + t]), perm[sw0 + t]);
+                for (int e = (kk - 2) / 2; e >= 0; e--) kheap_sift_down(K, e, kk, K[32 * e]);
+                rk = K[0];
+                for (int t = kk; t < ns; t++) {
+                    const float f = f_d2_fma(Q, pos[sw0 + t]);
+                    const uint64_t key = pack_key(f, perm[sw0 + t]);
+                    if (key < rk) {
+                        frej = fminf(frej, key_f(rk));
+                        kheap_sift_down(K, 0, kk, key);
+                        rk = K[0];
+                    } else {
+                        frej = fminf(frej, f);
+                    }
+                }
+                bf = key_f(rk);
+            }
+            // ---- the smallest subtree holding [qa, qb]
+            int c = owner[qa];
+            KnnNode C = nodes[c];
+            while (!(C.lstart <= qa && qb < C.lstart + C.count) && C.parent >= 0) {
+                c = C.parent;
+                C = nodes[c];
+            }
+            int w0 = c, w1 = C.skip, x0 = -1, x1 = -1;
+            double tbox;  // squared distance from the query to the outside of the processed box
+            while (true) {
+                int i = w0, wb = INT_MIN / 2;
+                while (i < w1) {
+                    if (i == x0) {
+                        i = x1;
+                        continue;
+                    }
+                    if (i >= wb + 32 || i < wb) {
+                        wb = i;
+                        const int nw = min(32, w1 - wb) * 12;
+                        __syncwarp();
+                        for (int t = lane; t < nw; t += 32) win_w[t] = nodes_w[(int64_t)wb * 12 + t];
+                        __syncwarp();
+                    }
+                    const float4 *nv = reinterpret_cast<const float4 *>(win + (i - wb));
+                    const float4 n0 = nv[0], n1 = nv[1];
+                    const float gx = fmaxf(fmaxf(n0.x - Q.x, Q.x - n0.w), 0.f);
+                    const float gy = fmaxf(fmaxf(n0.y - Q.y, Q.y - n1.x), 0.f);
+                    const float gz = fmaxf(fmaxf(n0.z - Q.z, Q.z - n1.y), 0.f);
+                    const float lb = __fmaf_rn(gx, gx, __fmaf_rn(gy, gy, __fmul_rn(gz, gz)));
+                    if (COUNT) ctr[0]++;
+                    if (!__any_sync(0xffffffffu, me && lb <= bf)) {
+                        frej = fminf(frej, lb);  // the whole subtree lies in this box
+                        i = __float_as_int(n1.z);
+                        continue;
+                    }
+                    const int l0 = __float_as_int(n1.w);
+                    const int l1 = l0 + __float_as_int(nv[2].x);
+                    for (int base = l0; base < l1; base += 32) {
+                        const int j = base + lane;
+                        __syncwarp();
+                        if (j < l1) {
+                            cpos[lane] = pos[j];
+                            cid[lane] = perm[j];
+                        }
+                        __syncwarp();
+                        const int m = min(32, l1 - base);
+                        if (COUNT) ctr[1] += m;
+                        // filter: a branch-free pass over the tile against
+                        // the bound at its start (the bound only tightens)
+                        unsigned pass = 0;
+#pragma unroll 4
+                        for (int t = 0; t < m; t++) {
+                            const float f = f_d2_fma(Q, cpos[t]);
+                            const int p = base + t;
+                            const bool seed = p >= sw0 && p < sw1;
+                            const bool ok = me && !seed && f <= bf;
+                            pass |= (unsigned)ok << t;
+                            frej = (ok || seed || !me) ? frej : fminf(frej, f);
+                        }
+                        if (COUNT) {
+                            ctr[3] += __reduce_max_sync(0xffffffffu, (unsigned)__popc(pass));
+                        }
+                        // insert the survivors (each lane its own)
+                        while (pass) {
+                            const int t = __ffs(pass) - 1;
+                            pass &= pass - 1;
+                            const float f = f_d2_fma(Q, cpos[t]);
+                            const uint64_t key = pack_key(f, cid[t]);
+                            if (key < rk) {
+                                frej = fminf(frej, bf);  // the evicted root
+                                kheap_sift_down(K, 0, kk, key);
+                                rk = K[0];
+                                bf = key_f(rk);
+                                if (COUNT) ctr[2]++;
+                            } else {
+                                frej = fminf(frej, f);
+                            }
+                        }
+                    }
+                    i++;
+                }
+                // distance from the query to the outside of C's box (exact
+                // differences of floats, squared in double)
+                const double dbx = fmin((double)Q.x - (double)C.lo[0], (double)C.hi[0] - (double)Q.x);
+                const double dby = fmin((double)Q.y - (double)C.lo[1], (double)C.hi[1] - (double)Q.y);
+                const double dbz = fmin((double)Q.z - (double)C.lo[2], (double)C.hi[2] - (double)Q.z);
+                const double db = fmin(fmin(dbx, dby), dbz);
+                tbox = C.parent < 0 ? kInf : (db > 0.0 ? db * db : 0.0);
+                const bool done = !me || tbox > (double)bf * (1.0 + 4e-6);
+                if (C.parent < 0 || __all_sync(0xffffffffu, done)) break;
+                const int a = C.parent;
+                const KnnNode A = nodes[a];
+                w0 = a;
+                w1 = A.skip;
+                x0 = c;
+                x1 = C.skip;
+                c = a;
+                C = A;
+            }
+            // certification threshold: a lower bound of the exact distance^2
+            // of every particle not kept
+            const double tcert = fmin((double)frej * (1.0 - 2e-6), tbox * (1.0 - 1e-12));
+            // ---- transpose the heaps: entry e of lane l moves to slot
+            // 32 e + (l ^ e), so that the warp reads one lane's column
+            // without bank conflicts
+            for (int e = 0; e < kk; e++) {
+                const uint64_t v = KH[32 * e + lane];
+                __syncwarp();
+                KH[32 * e + (lane ^ e)] = v;
+                __syncwarp();
+            }
+            // ---- one query at a time: exact FP64 re-rank, certify, write
+            for (unsigned mm = act; mm; mm &= mm - 1) {
+                const int r = __ffs(mm) - 1;
+                float4 Qr;
+                Qr.x = __shfl_sync(0xffffffffu, Q.x, r);
+                Qr.y = __shfl_sync(0xffffffffu, Q.y, r);
+                Qr.z = __shfl_sync(0xffffffffu, Q.z, r);
+                const double tr = __shfl_sync(0xffffffffu, tcert, r);
+                const int rid = __shfl_sync(0xffffffffu, myid, r);
+                int id = INT_MAX;
+                double d = kInf;
+                if (lane < kk) {
+                    id = (int)(uint32_t)KH[32 * lane + (r ^ lane)];
+                    d = exact_d2(Qr, pos_batch[id]);
+                }
+                warp_sort(d, id);
+                const double dk = __shfl_sync(0xffffffffu, d, kk - 1);
+                if (dk < tr) {
+                    if (lane < k) nearindex[(int64_t)rid * k + lane] = lane < kk ? (int32_t)(id - hs) : -1;
+                    // nnost.c:292,415: maxr = sqrtf(maxdist2); W4(sqrtf(d2_j), maxr/2.)
+                    const float neardist = sqrtf((float)dk);
+                    const float hh = (float)(neardist / 2.);
+                    const float wj = lane < kk ? w4(sqrtf((float)d), hh) : 0.f;
+                    float rho = 0.f;
+                    for (int j = 0; j < kk; j++) rho += __shfl_sync(0xffffffffu, wj, j);
+                    if (lane == 0 && dens) dens[rid] = rho;
+                } else if (lane == 0) {
+                    redo[atomicAdd(nredo, 1u)] = (int32_t)(b + r);
+                    if (COUNT) ctr[4]++;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (COUNT && counters) {
+        for (int off = 16; off; off >>= 1) ctr[2] += __shfl_xor_sync(0xffffffffu, ctr[2], off);
+        if (lane == 0) {
+            atomicAdd(counters + 0, ctr[0]);
+            atomicAdd(counters + 1, ctr[1]);
+            atomicAdd(counters + 2, ctr[2]);
+            atomicAdd(counters + 3, ctr[3]);
+            atomicAdd(counters + 4, ctr[4]);
+        }
+    }
+}
+
 }  // namespace
 
 int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const float4 *pos_batch, int k,
@@ -733,6 +1009,32 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
     }
     const int64_t nquery = qlist ? nq : t.n;
     if (t.n <= 0 || nquery <= 0) return GF_OK;
+    if (GF_KNN_ALGO == 2 && !qlist) {
+        // scratch: the list of queries the float-key kernel could not certify
+        GF_TRY(ctx->tmp[7].reserve((size_t)t.n * sizeof(int32_t) + 256));
+        unsigned *nredo = ctx->tmp[7].as<unsigned>();
+        int32_t *redo = reinterpret_cast<int32_t *>(ctx->tmp[7].as<char>() + 256);
+        GF_CUDA_TRY(cudaMemsetAsync(nredo, 0, sizeof(unsigned), ctx->stream));
+        const int block = GF_KNNB_BLOCK;
+        const size_t shmem = (size_t)(block / 32) * kFBucketWarpBytes;
+        int per_sm = 0;
+        auto kern = counters ? knn_fbucket_kernel<true> : knn_fbucket_kernel<false>;
+        GF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+        GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, shmem));
+        const int64_t nbucket = (t.n + 31) / 32;
+        int64_t grid = (nbucket * 32 + block - 1) / block;
+        grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * std::max(per_sm, 1)));
+        kern<<<(int)grid, block, shmem, ctx->stream>>>(t.n, k, t.pos, t.perm, pos_batch, t.phalo, pstart, t.owner,
+                                                       t.knn, nearindex, dens, redo, nredo, counters);
+        GF_LAUNCH_CHECK();
+        // the uncertified queries, exactly, into their own rows (the count
+        // stays on the device; the grid strides over whatever it is)
+        knn_kernel<false><<<148 * (2048 / GF_KNN_BLOCK), GF_KNN_BLOCK, 0, ctx->stream>>>(
+            t.n, k, t.pos, t.perm, pos_batch, t.phalo, pstart, t.owner, t.knn, nearindex, dens, ctx->d_err,
+            nullptr, redo, nredo, true);
+        GF_LAUNCH_CHECK();
+        return GF_OK;
+    }
     if (GF_KNN_ALGO == 1 && !qlist) {
         const int block = GF_KNNB_BLOCK;
         const size_t shmem = (size_t)(block / 32) * kBucketWarpBytes;

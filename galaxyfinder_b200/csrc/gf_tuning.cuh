@@ -14,8 +14,8 @@
 #define GF_KNN_CHUNK 32
 #endif
 #ifndef GF_KNN_ALGO    // 1: bucket kNN (a warp walks once for 32 tree-order queries,
-#define GF_KNN_ALGO 1  //    lane = query); 0: one warp per query
-#endif
+#define GF_KNN_ALGO 1  //    lane = query); 2: the same with float heap keys and an
+#endif                 //    exact certification; 0: one warp per query
 #ifndef GF_KNNB_BLOCK  // threads per block of knn_bucket_kernel (14.5 KB shared memory per warp)
 #define GF_KNNB_BLOCK 32
 #endif
@@ -41,7 +41,7 @@
 static_assert(GF_KNN_BLOCK % 32 == 0 && GF_KNN_BLOCK <= 1024, "GF_KNN_BLOCK");
 static_assert(GF_KNN_CHUNK >= 1, "GF_KNN_CHUNK");
 static_assert(GF_KNNB_BLOCK % 32 == 0 && GF_KNNB_BLOCK <= 512, "GF_KNNB_BLOCK");
-static_assert(GF_KNN_ALGO == 0 || GF_KNN_ALGO == 1, "GF_KNN_ALGO");
+static_assert(GF_KNN_ALGO >= 0 && GF_KNN_ALGO <= 2, "GF_KNN_ALGO");
 static_assert(GF_KNNB_ARITY == 2 || GF_KNNB_ARITY == 4, "GF_KNNB_ARITY");
 static_assert(GF_BH_BLOCK % 32 == 0 && GF_BH_BLOCK <= 1024, "GF_BH_BLOCK");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");

@@ -11,7 +11,7 @@ result goes to galaxyfinder_b200/tuned.json (parameters, every measurement,
 the GPU and the workload), which build.py turns into -D flags.
 
   group   parameters                                   phase
-  knn     GF_KNN_ALGO x GF_KNNB_BLOCK x GF_KNNB_ARITY; for the warp-per-query
+  knn     GF_KNN_ALGO x GF_KNNB_BLOCK (x GF_KNNB_ARITY); for the warp-per-query
           kernel GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
   bh      GF_BH_BLOCK, then the register cap           potential
   fft     GF_FFT_PENCILS                               smooth
@@ -49,10 +49,11 @@ def minb(block: int, regs: int) -> int:
 # overrides (an empty list skips the stage)
 def stages(group: str):
     if group == "knn":
-        return [lambda base: [{"GF_KNN_ALGO": 1, "GF_KNNB_BLOCK": b, "GF_KNNB_ARITY": a}
-                              for b in (32, 64) for a in (2, 4)] + [{"GF_KNN_ALGO": 0}],
-                lambda base: [] if base["GF_KNN_ALGO"] == 1 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
-                lambda base: [] if base["GF_KNN_ALGO"] == 1 else
+        return [lambda base: [{"GF_KNN_ALGO": a, "GF_KNNB_BLOCK": b, "GF_KNNB_ARITY": 2}
+                              for a in (1, 2) for b in (32, 64)] +
+                [{"GF_KNN_ALGO": 1, "GF_KNNB_BLOCK": 32, "GF_KNNB_ARITY": 4}, {"GF_KNN_ALGO": 0}],
+                lambda base: [] if base["GF_KNN_ALGO"] != 0 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
+                lambda base: [] if base["GF_KNN_ALGO"] != 0 else
                 [{"GF_KNN_BLOCK": b, "GF_KNN_MINB": minb(b, r)} for b in (128, 256) for r in REGCAPS]]
     if group == "bh":
         return [lambda base: [{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],

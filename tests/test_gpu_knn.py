@@ -77,6 +77,29 @@ def test_knn_ties_broken_by_index(restatement, ctx):
     np.testing.assert_array_equal(near.cpu().numpy(), idx)
 
 
+def test_knn_lattice_shells(restatement, ctx):
+    """A cubic lattice with power-of-two spacing: every distance is exact and
+    comes in shells of 6, 12, 8, ... equal distances, so the k-th place falls
+    inside a tie group for almost every query (the float-key kernel cannot
+    certify those and hands them to the exact kernel).  Batched with a random
+    halo of the same size."""
+    g = np.arange(12, dtype=np.float32) * np.float32(2.0 ** -7)
+    lat = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.default_rng(5)
+    lat = lat[rng.permutation(len(lat))]
+    rnd = (rng.random((len(lat), 3)) * 0.1).astype(np.float32)
+    k = 32
+    pos4 = np.concatenate([np.concatenate([p, np.ones((len(p), 1), np.float32)], 1) for p in (lat, rnd)])
+    ps = [0, len(lat), 2 * len(lat)]
+    near, dens = batch.knn_density(ctx, ps, pos4, k)
+    near, dens = near.cpu().numpy(), dens.cpu().numpy()
+    for h, p in enumerate((lat, rnd)):
+        a, b = ps[h], ps[h + 1]
+        idx, d2 = restatement.knn(p[:, 0], p[:, 1], p[:, 2], k, "brute")
+        np.testing.assert_array_equal(near[a:b], idx, err_msg=f"halo {h}")
+        np.testing.assert_array_equal(dens[a:b], restatement.sph_density(d2), err_msg=f"halo {h}")
+
+
 def test_tree_structure_invariants(ctx):
     hb = synth.catalogue(seed=5, nhalo=6, nmin=100, nmax=50000)
     pos = [_recentred_fp32(hb, h) for h in range(hb.nhalo)]

@@ -7,7 +7,7 @@ from galaxyfinder_b200 import tune as T
 
 
 def _valid(p):
-    assert p["GF_KNN_ALGO"] in (0, 1)
+    assert p["GF_KNN_ALGO"] in (0, 1, 2)
     assert p["GF_KNNB_BLOCK"] % 32 == 0 and p["GF_KNNB_BLOCK"] <= 512
     assert p["GF_KNN_BLOCK"] % 32 == 0 and p["GF_KNN_BLOCK"] <= 1024
     assert p["GF_BH_BLOCK"] % 32 == 0 and p["GF_BH_BLOCK"] <= 1024
@@ -19,7 +19,7 @@ def _valid(p):
 
 def test_search_space_is_valid():
     # both kNN kernels: the warp-per-query stages open up when it wins
-    for algo in (0, 1):
+    for algo in (0, 1, 2):
         base = dict(T.DEFAULTS, GF_KNN_ALGO=algo)
         for g in T.GROUPS:
             nonempty = 0
