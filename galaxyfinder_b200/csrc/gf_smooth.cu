@@ -264,22 +264,27 @@ __device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, fl
     // the 8 consecutive padded slots 9p .. 9p + 7.
     constexpr int OUT_STRIDE = S >= 8 ? S + S / 8 : 1;
     static_assert(S >= 8 || R == 8, "the first pass is radix 8");
+    // In the last pass (S R == N) p is always 0: every twiddle is w^0 = 1,
+    // and multiplying by (1, 0) returns its operand exactly, so it is skipped.
+    constexpr bool LAST = S * R == N;
     for (int e = threadIdx.x; e < npair * ITEMS; e += blockDim.x) {
         const int c = e / ITEMS;  // ITEMS is a power of two
         const int t = e - c * ITEMS;
-        const int q = t % S;
-        const int p = t / S;
+        const int q = LAST ? t : t % S;
+        const int p = LAST ? 0 : t / S;
         const int k0 = q + S * p;
         const float2 *x = src + c * L::SN + k0 + (k0 >> 3);
         float2 a[R];
 #pragma unroll
         for (int r = 0; r < R; r++) a[r] = x[r * IN_STRIDE];
         dft<R, INV>(a);
+        if (!LAST) {
 #pragma unroll
-        for (int j = 1; j < R; j++) {
-            float2 w = tw[(p * S * j) & (N - 1)];
-            if (INV) w.y = -w.y;
-            a[j] = cmul(a[j], w);
+            for (int j = 1; j < R; j++) {
+                float2 w = tw[(p * S * j) & (N - 1)];
+                if (INV) w.y = -w.y;
+                a[j] = cmul(a[j], w);
+            }
         }
         const int kb = q + S * R * p;
         float2 *y = dst + c * L::SN + kb + (kb >> 3);
