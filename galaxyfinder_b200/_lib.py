@@ -185,6 +185,11 @@ SIGNATURES = {
     "gf_find_den_adjoint": (_INT, [_VP, ctypes.POINTER(Batch), _VP, _VP, _VP, _VP, _VP, _VP,
                                    _VP]),
     "gf_refine_centres": (_INT, [_VP, _I32, _VP, _VP, _I32, _VP, _VP, _VP, _VP, _INT, _D, _VP, _VP]),
+    "gf_density_peaks": (_INT, [_VP, _I32, _INT, _VP, _VP, _VP, _D, _I32, _VP, _VP]),
+    "gf_core_density": (_INT, [_VP, _I32, _INT, _VP, _VP, _VP, _VP, _I32, _VP, _VP, _VP, _VP, _VP, _VP,
+                               _VP]),
+    "finddenpeak": (_INT, [_VP, _INT, _VP, _INT, _VP, _INT, _VP]),
+    "FindCoreDensity": (_INT, [_VP, _INT, _VP, _INT, _VP, _INT]),
     "gf_mesh_peaks": (_INT, [_VP, _I32, _VP, _VP, _VP, _INT, _F, _I64, _VP, _VP, _VP,
                              ctypes.POINTER(_I64)]),
     "gf_self_potential": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _I32, _D, _INT, _VP, _VP]),

@@ -216,6 +216,38 @@ def stage_run(ctx: Context, batch: DeviceBatch, cfg: _lib.StageConfig,
     return out
 
 
+def density_peaks(ctx: Context, den, neighbor, type_=None, threshold=2000.0):
+    """finddenpeak's peaks (subhaloden.mod6.c:416-494) of one halo on the
+    device: den (np,) float32, neighbor (np, k) int32 halo-local kNN lists,
+    type_ (np,) int32 to keep stars only.  Returns the peak indices (int32
+    device tensor, particle order)."""
+    np_, k = neighbor.shape
+    peak = torch.empty(max(np_, 1), dtype=torch.int32, device=den.device)
+    npeak = ctypes.c_int32()
+    check(lib().gf_density_peaks(ctx.handle, np_, k, ptr(den), ptr(neighbor), ptr(type_), threshold,
+                                 np_, ptr(peak), ctypes.byref(npeak)))
+    return peak[:npeak.value]
+
+
+def core_density(ctx: Context, den, neighbor, type_, mass, peak):
+    """FindCoreDensity (subhaloden.mod6.c:1167-1475) of one halo on the device:
+    per core its core density, member and star counts and star mass, per
+    particle its core id (-9999 for none) and working-particle flag."""
+    np_, k = neighbor.shape
+    nc = int(peak.numel())
+    dev = den.device
+    out = dict(coredensity=torch.empty(nc, dtype=torch.float32, device=dev),
+               nummem=torch.empty(nc, dtype=torch.int32, device=dev),
+               numstar=torch.empty(nc, dtype=torch.int32, device=dev),
+               starmass=torch.empty(nc, dtype=torch.float32, device=dev),
+               haloid=torch.empty(np_, dtype=torch.int32, device=dev),
+               flag=torch.empty(np_, dtype=torch.uint8, device=dev))
+    check(lib().gf_core_density(ctx.handle, np_, k, ptr(den), ptr(neighbor), ptr(type_), ptr(mass), nc,
+                                ptr(peak), *(ptr(out[f]) for f in ("coredensity", "nummem", "numstar",
+                                                                  "starmass", "haloid", "flag"))))
+    return out
+
+
 class PipelinedStage:
     """The stage over a catalogue split into halo chunks of similar particle
     counts, each with its own context, CUDA stream, device buffers and host

@@ -163,6 +163,21 @@ def lagFindStellarCore(bp, numnear, ptype=_lib.TYPE_ALL, maxnumcore=100000):
     return dens, cores[:ncore.value].copy(), near
 
 
+def finddenpeak(den, neighbor, bp, jflag=0, maxnumcore=1000000):
+    """subhaloden.mod6.c:416 — density peaks on the kNN graph as cores
+    (CORE_DTYPE: peak, cx, cy, cz, density filled), in particle order.  jflag 1
+    keeps stellar peaks only."""
+    bp = _bp(bp)
+    den = np.ascontiguousarray(den, np.float32)
+    nb = np.ascontiguousarray(neighbor, np.int64)
+    n, k = nb.shape
+    cores = np.zeros(max(maxnumcore, 1), _lib.CORE_DTYPE)
+    cptr = _lib.ctypes.c_void_p(cores.ctypes.data)
+    nc = lib().finddenpeak(ptr(den), k, ptr(nb), n, _lib.ctypes.byref(cptr), jflag, ptr(bp))
+    check_last()
+    return cores[:nc].copy()
+
+
 def i_potent_spline():
     """force_spline.mod3.c:81 — no table is needed by the GPU kernel."""
     lib().i_potent_spline()

@@ -100,6 +100,24 @@ void findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, i
 void lagFindStellarCore(SimpleBasicParticleType *bp, int np, int Numnear, float *densph,
                         Coretype **Core, int *NumCore, int maxnumcore, long long *nearindex,
                         int ptype);
+/* NewGalFinder/subhaloden.mod6.c:416.  Density peaks on the kNN graph:
+ * particles with den > PEAKTHRESHOLD (stars only when jflag is 1) whose kNN
+ * list (neighbor, np*numneigh) holds no denser particle, written to *Core in
+ * particle order (peak, cx, cy, cz, density); returns their number.  The
+ * caller's array holds MAXNUMCORE cores; more peaks grow it by MAXNUMCORE
+ * through the reference's arena Realloc (the reference's static maxnumcore is
+ * not updated).  More than MAXNUMCORE peaks on the all-particle path exit
+ * with 999, as the reference does (GF_ERANGE with GF_NOEXIT). */
+int finddenpeak(float *den, int numneigh, long long *neighbor, int np, Coretype **Core, int jflag,
+                SimpleBasicParticleType *bp);
+/* NewGalFinder/subhaloden.mod6.c:1167.  Core density and core members of each
+ * core on the kNN graph (see gf_core_density).  Reads the densities from and
+ * writes haloid and flag to the reference's working-particle array wp,
+ * resolved when libgf is linked into the reference program (GF_ENOTIMPL
+ * otherwise); fills coredensity, nummem, numstar and starmass of core[].
+ * Returns numcore. */
+int FindCoreDensity(SimpleBasicParticleType *bp, int np, long long *neighbor, int NumNeighbor,
+                    Coretype *core, int numcore);
 /* NewGalFinder/subhaloden.mod6.c:1477 */
 void Self_Halo_Potent(int np, Vector3d *r, float *mass, float *penergy);
 /* NewGalFinder/subhaloden.mod6.c:1537 */
@@ -248,6 +266,33 @@ int gf_find_den_adjoint(gf_ctx *ctx, const gf_batch *b, const gf_mesh_desc *mesh
 int gf_refine_centres(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_dev, const float *den,
                       int32_t ncentre, const int32_t *halo_dev, double *cx, double *cy, double *cz,
                       int max_steps, double step_frac, double *rho, int32_t *moves);
+
+/* Density peaks of one halo's kNN graph (finddenpeak,
+ * NewGalFinder/subhaloden.mod6.c:416-494): particles with den > threshold
+ * (and type == GF_TYPE_STAR when type is not NULL) whose kNN list holds no
+ * denser particle.  den (np), neighbor (np*numneighbor, halo-local int32) and
+ * type are device arrays; up to cap peak indices go to peak (device) in
+ * particle order; *npeak (host) receives the number found (GF_ERANGE when it
+ * exceeds cap). */
+int gf_density_peaks(gf_ctx *ctx, int32_t np, int numneighbor, const float *den, const int32_t *neighbor,
+                     const int32_t *type, double threshold, int32_t cap, int32_t *peak, int32_t *npeak);
+/* Core densities and core members (FindCoreDensity,
+ * NewGalFinder/subhaloden.mod6.c:1167-1475), all arrays on the device: per
+ * core c (peak[c]) the density threshold is bisected between den[peak] and
+ * max(DENFLOOR, min den) until |(up - down)/t| <= COREDENRESOLUTION, a trial
+ * t failing when a breadth-first search from the peak along kNN edges through
+ * particles with den > t reaches another peak; coredensity[c] = up, and the
+ * particles reached at up are the members (none if another peak is reached):
+ * nummem, numstar (GF_TYPE_STAR members), starmass (their mass, summed in
+ * FP64 and rounded to float; the reference adds in float in its search
+ * order).  haloid[i] = the highest core index that reached i, -9999
+ * (NOT_HALO_MEMBER) for none; flag[i] = PEAK (0x01) for peaks | CORE|BOUND
+ * (0x14) for members.  Uses up to about 1 GiB of scratch for concurrent
+ * searches. */
+int gf_core_density(gf_ctx *ctx, int32_t np, int numneighbor, const float *den, const int32_t *neighbor,
+                    const int32_t *type, const double *mass, int32_t ncore, const int32_t *peak,
+                    float *coredensity, int32_t *nummem, int32_t *numstar, float *starmass, int32_t *haloid,
+                    uint8_t *flag);
 
 /* Strict 26-neighbour maxima of every mesh above threshold, in the interior
  * [margin, n - margin) of each axis (the mesh peak test of nnost.c:1176-1200;

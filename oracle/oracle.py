@@ -178,6 +178,9 @@ class Reference:
                                               _VP, _VP, _VP, _VP]
             L.ref_AdGetTidalRCenterCore.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP, _I, _VP,
                                                     _VP, _VP]
+            L.ref_finddenpeak.argtypes = [_I, _VP, _VP, _I, _VP, _VP, _VP, _VP, _I, _I, _VP, _VP]
+            L.ref_FindCoreDensity.argtypes = [_I, _VP, _VP, _I, _VP, _VP, _I, _VP, _VP, _VP, _VP, _VP,
+                                              _VP, _VP]
             if L.ref_init(arena_mb) != 0:
                 raise RuntimeError("reference arena allocation failed")
             Reference._libs[variant] = L
@@ -307,6 +310,37 @@ class Reference:
         self.L.ref_AdGetTidalRCenterCore(len(x), _p(x), _p(y), _p(z), _p(mass), _p(hid), nc,
                                          _p(c6), len(sc), _p(sc), _p(rt), _p(nm))
         return rt, nm
+
+    def finddenpeak(self, den, neighbor, type_, x, y, z, jflag=0):
+        """subhaloden.mod6.c:416 -> (peak particles, (npeak, 4) float cx, cy, cz, density)."""
+        den = np.ascontiguousarray(den, np.float32)
+        nb = np.ascontiguousarray(neighbor, np.int64)
+        t = np.ascontiguousarray(type_, np.int32)
+        x, y, z = map(self._d, (x, y, z))
+        n, k = nb.shape
+        peak = np.zeros(max(n, 1), np.int32)
+        xyzd = np.zeros(4 * max(n, 1), np.float32)
+        nc = self.L.ref_finddenpeak(n, _p(den), _p(nb), k, _p(t), _p(x), _p(y), _p(z), jflag, n,
+                                    _p(peak), _p(xyzd))
+        return peak[:nc], xyzd[:4 * nc].reshape(nc, 4)
+
+    def FindCoreDensity(self, den, neighbor, type_, mass, peak):
+        """subhaloden.mod6.c:1167, one thread -> dict of per-core coredensity,
+        nummem, numstar, starmass and per-particle haloid, flag."""
+        den = np.ascontiguousarray(den, np.float32)
+        nb = np.ascontiguousarray(neighbor, np.int64)
+        t = np.ascontiguousarray(type_, np.int32)
+        m = self._d(mass)
+        pk = np.ascontiguousarray(peak, np.int32)
+        n, k = nb.shape
+        nc = len(pk)
+        out = dict(coredensity=np.zeros(nc, np.float32), nummem=np.zeros(nc, np.int32),
+                   numstar=np.zeros(nc, np.int32), starmass=np.zeros(nc, np.float32),
+                   haloid=np.zeros(n, np.int32), flag=np.zeros(n, np.uint8))
+        self.L.ref_FindCoreDensity(n, _p(den), _p(nb), k, _p(t), _p(m), nc, _p(pk),
+                                   *(_p(out[f]) for f in ("coredensity", "nummem", "numstar",
+                                                          "starmass", "haloid", "flag")))
+        return out
 
     def subhalo_den(self, x, y, z, vx, vy, vz, mass, type_):
         """subhaloden.mod6.c:2861 on one FoF halo -> (result, p2halo)."""

@@ -328,6 +328,64 @@ int ref_AdGetTidalRCenterCore(int np, const double *x, const double *y, const do
     return 0;
 }
 
+/* ---- core finding on the kNN graph (subhaloden.mod6.c:416-494, 1167-1475) ---- */
+int finddenpeak(float *, int, long long *, int, Coretype **, int, SimpleBasicParticleType *);
+int FindCoreDensity(SimpleBasicParticleType *, int, long long *, int, Coretype *, int);
+void omp_set_num_threads(int);
+int omp_get_max_threads(void);
+
+/* finddenpeak on given densities and kNN lists; peak[] receives the peak
+ * particles in the reference's order, xyzd[4 c] their float cx, cy, cz and
+ * density.  Returns the number of peaks (at most maxcore are written). */
+int ref_finddenpeak(int np, const float *den, const long long *neighbor, int numneigh, const int *type,
+                    const double *x, const double *y, const double *z, int jflag, int maxcore,
+                    int *peak, float *xyzd) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, type, x, y, z, NULL);
+    Coretype *core = NULL;
+    core = (Coretype *)Malloc(sizeof(Coretype) * (size_t)MAXNUMCORE, PPTR(core));
+    int nc = finddenpeak((float *)den, numneigh, (long long *)neighbor, np, &core, jflag, bp);
+    for (int c = 0; c < nc && c < maxcore; c++) {
+        peak[c] = core[c].peak;
+        xyzd[4 * c] = core[c].cx; xyzd[4 * c + 1] = core[c].cy;
+        xyzd[4 * c + 2] = core[c].cz; xyzd[4 * c + 3] = core[c].density;
+    }
+    Free(core);
+    Free(bp);
+    return nc;
+}
+
+/* FindCoreDensity on one thread (its member ids then follow the core order)
+ * for the given densities, kNN lists and core peaks.  Outputs per core
+ * (coredensity, nummem, numstar, starmass) and per particle (haloid, flag). */
+int ref_FindCoreDensity(int np, const float *den, const long long *neighbor, int numneigh,
+                        const int *type, const double *mass, int numcore, const int *peak,
+                        float *coredensity, int *nummem, int *numstar, float *starmass,
+                        int *haloid, unsigned char *flag) {
+    if (!g_ready) return -1;
+    double *zero = (double *)calloc((size_t)(np > 0 ? np : 1), sizeof(double));
+    SimpleBasicParticleType *bp = make_bp(np, type, zero, zero, zero, mass);
+    WorkingParticle_h *w = (WorkingParticle_h *)calloc((size_t)(np > 0 ? np : 1), sizeof(WorkingParticle_h));
+    for (int i = 0; i < np; i++) w[i].den = den[i];
+    WorkingParticle_h *saved = wp;
+    wp = w;
+    Coretype *core = (Coretype *)calloc((size_t)(numcore > 0 ? numcore : 1), sizeof(Coretype));
+    for (int c = 0; c < numcore; c++) core[c].peak = peak[c];
+    int nth = omp_get_max_threads();
+    omp_set_num_threads(1);
+    int r = FindCoreDensity(bp, np, (long long *)neighbor, numneigh, core, numcore);
+    omp_set_num_threads(nth);
+    for (int c = 0; c < numcore; c++) {
+        coredensity[c] = core[c].coredensity; nummem[c] = core[c].nummem;
+        numstar[c] = core[c].numstar; starmass[c] = core[c].starmass;
+    }
+    for (int i = 0; i < np; i++) { haloid[i] = w[i].haloid; flag[i] = w[i].flag; }
+    wp = saved;
+    free(core); free(w); free(zero);
+    Free(bp);
+    return r;
+}
+
 /* ---- the reference's per-halo pipeline (subhaloden.mod6.c:2861) ---- */
 int subhalo_den(FoFTPtlStruct *, int, int *); /* lint is int, header.h:74 */
 

@@ -112,8 +112,28 @@ def main():
                         r1kineticfact=r1k, r2kineticfact=r2k,
                         bg_1e12=ref.bg_potent(1e12), bg_mass=ref.bg_potent(float(np.sum(mf, dtype=np.float64))))
     bound_fixture(ref)
+    cores_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
+
+
+def cores_fixture(ref):
+    """finddenpeak (subhaloden.mod6.c:416; all particles and stars only) and
+    FindCoreDensity (:1167) on the reference's own kNN lists and SPH
+    densities (findsphdensity) of a clustered halo with four clumps."""
+    n = 3000
+    p = blob(21, n, 0.02, nsub=4)
+    rng = np.random.default_rng(21)
+    mass = 10 ** rng.uniform(6, 8, n)
+    typ = np.where(rng.random(n) < 0.3, 1, 2).astype(np.int32)
+    idx, dens = ref.findsphdensity(p[:, 0], p[:, 1], p[:, 2], mass, 32)
+    peak, xyzd = ref.finddenpeak(dens, idx, typ, p[:, 0], p[:, 1], p[:, 2], 0)
+    speak, sxyzd = ref.finddenpeak(dens, idx, typ, p[:, 0], p[:, 1], p[:, 2], 1)
+    cd = ref.FindCoreDensity(dens, idx, typ, mass, peak)
+    out = dict(pos=p, mass=mass, type=typ, neighbor=idx.astype(np.int16), den=dens, peak=peak,
+               peak_xyzd=xyzd, star_peak=speak, star_peak_xyzd=sxyzd)
+    out.update({f"core_{k}": v for k, v in cd.items()})
+    np.savez_compressed(OUT / "cores.npz", **out)
 
 
 def clumps(rng, sizes, centres, sigmas):
@@ -190,4 +210,8 @@ def bound_fixture(ref):
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1:  # named fixtures only, e.g. `make_golden.py cores`
+        for name in sys.argv[1:]:
+            globals()[f"{name}_fixture"](Reference("fixed"))
+    else:
+        main()
