@@ -239,7 +239,7 @@ def main():
         dist.init_process_group("nccl" if args.impl == "gf" else "gloo",
                                 timeout=datetime.timedelta(seconds=600))
 
-    from galaxyfinder_b200 import _lib, batch, synth
+    from galaxyfinder_b200 import _lib, batch, shard, synth
 
     mesh_rule = batch.mesh_rule(mode=_lib.MESH_POW2, nmin=64, nmax=256, rg=2.0, rg_in_cells=True)
     base = {"metric": METRIC, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -273,18 +273,10 @@ def main():
             dist.barrier()
 
     def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return v if dist is None else shard.max_over_ranks(v, device=dev)
 
     def sum_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return v if dist is None else shard.sum_over_ranks(v, device=dev)
 
     # ---- warm-up
     for _ in range(max(args.warmup, 3)):
