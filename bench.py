@@ -44,7 +44,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per particle of
 # each phase's dominant kernel, from one ncu capture of the 256-halo catalogue
 # (201,933 particles); the traffic scales with the particles processed.
-TRAFFIC_PER_PARTICLE = {"knn": (6.209024e6 + 2.816e3) / 201933}
+TRAFFIC_PER_PARTICLE = {"knn": (9.437952e6 + 1.28e3) / 201933}
 
 
 def parse():
@@ -353,14 +353,13 @@ def main():
     pipe_res = {}
     for mode in ("resident", "e2e"):
         runner = pipe.run_resident if mode == "resident" else pipe.run_e2e
-        for _ in range(max(args.warmup, 3)):
-            runner()
+        runner(max(args.warmup, 3))
         torch.cuda.synchronize()
         barrier()
         l0 = lib.gf_kernel_launch_count()
-        spans = [runner() for _ in range(args.steps)]
+        p0, p1 = runner(args.steps)  # each chunk streams its K passes back to back
         torch.cuda.synchronize()
-        pms = max_over_ranks(spans[0][0].elapsed_time(spans[-1][1]) / args.steps)
+        pms = max_over_ranks(p0.elapsed_time(p1) / args.steps)
         pipe_res[mode] = {"value": total_particles / (pms / 1e3), "ms_per_step": pms,
                           "launches": (lib.gf_kernel_launch_count() - l0) // max(args.steps, 1)}
     clk = clocks.stop()
@@ -446,7 +445,8 @@ def main():
                    "pipeline": f"{nchunks} halo chunks on their own streams and host threads"},
         "e2e": {"value": pipe_res["e2e"]["value"], "unit": UNIT, "h2d_bytes_per_step": pipe_h2d,
                 "d2h_bytes_per_step": pipe_d2h, "ms_per_step": pipe_res["e2e"]["ms_per_step"],
-                "path": "PipelinedStage.run_e2e: pinned host inputs in, all outputs back to pinned host"},
+                "path": "PipelinedStage.run_e2e(K): pinned host inputs in, all outputs back to pinned host, "
+                        "every pass; each chunk streams its K passes back to back"},
         "single_stream": {"value": value, "ms_per_step": ms, "gpu_launches": int(launches),
                           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                                   "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},

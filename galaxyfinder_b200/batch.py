@@ -260,10 +260,11 @@ class PipelinedStage:
     next chunk's kernels; the first chunks finish early and their outputs
     travel back while the later ones compute.
 
-    run_resident() runs every chunk on inputs already on the device;
-    run_e2e() also copies each chunk's inputs from pinned host memory and its
-    outputs back, inside the same overlapped schedule.  Both return the
-    (start, end) CUDA events that bracket all chunks."""
+    run_resident(steps) runs every chunk `steps` times on inputs already on
+    the device; run_e2e(steps) also copies each chunk's inputs from pinned
+    host memory and its outputs back every time, inside the same overlapped
+    schedule.  Both return the (start, end) CUDA events that bracket all
+    chunks' passes."""
 
     def __init__(self, hb, cfg: _lib.StageConfig, nchunk: int = 3, device: int = 0, k: int = 32,
                  prioritise: bool = True):
@@ -305,37 +306,40 @@ class PipelinedStage:
         self.h2d_bytes = sum(t.numel() * t.element_size() for c in self.chunks for t in c["host"].values())
         self.d2h_bytes = sum(t.numel() * t.element_size() for c in self.chunks for t in c["hout"].values())
 
-    def _chunk(self, c, e2e: bool, start):
+    def _chunk(self, c, e2e: bool, start, steps: int):
         s = c["stream"]
         s.wait_event(start)
-        if e2e:
-            with torch.cuda.stream(s):
-                for f in ("x", "y", "z", "mass", "type", "pstart"):
-                    getattr(c["db"], f).copy_(c["host"][f], non_blocking=True)
-        stage_run(c["ctx"], c["db"], self.cfg, c["out"])
-        if e2e:
-            with torch.cuda.stream(s):
-                for f, t in c["hout"].items():
-                    t.copy_(getattr(c["out"], f), non_blocking=True)
+        for _ in range(steps):  # this chunk's steps back to back on its stream
+            if e2e:
+                with torch.cuda.stream(s):
+                    for f in ("x", "y", "z", "mass", "type", "pstart"):
+                        getattr(c["db"], f).copy_(c["host"][f], non_blocking=True)
+            stage_run(c["ctx"], c["db"], self.cfg, c["out"])
+            if e2e:
+                with torch.cuda.stream(s):
+                    for f, t in c["hout"].items():
+                        t.copy_(getattr(c["out"], f), non_blocking=True)
         done = torch.cuda.Event()
         done.record(s)
         return done
 
-    def _run(self, e2e: bool):
+    def _run(self, e2e: bool, steps: int):
         cur = torch.cuda.current_stream()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(cur)
-        dones = list(self.pool.map(lambda c: self._chunk(c, e2e, start), self.chunks))
+        dones = list(self.pool.map(lambda c: self._chunk(c, e2e, start, steps), self.chunks))
         for d in dones:
             cur.wait_event(d)
         end.record(cur)
         return start, end
 
-    def run_resident(self):
-        return self._run(False)
+    def run_resident(self, steps: int = 1):
+        """`steps` passes over the catalogue; each chunk runs its passes back
+        to back, so one chunk's next pass overlaps another's current one."""
+        return self._run(False, steps)
 
-    def run_e2e(self):
-        return self._run(True)
+    def run_e2e(self, steps: int = 1):
+        return self._run(True, steps)
 
     def close(self):
         self.pool.shutdown()

@@ -315,10 +315,11 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
            const KnnNode *__restrict__ nodes, int32_t *__restrict__ nearindex,
            float *__restrict__ dens, int *err, unsigned long long *__restrict__ counters,
            const int32_t *__restrict__ qlist, const unsigned *__restrict__ nq_dev = nullptr,
-           bool natural_rows = false) {
+           bool natural_rows = false, int chunk = kChunk) {
     // nq_dev: the query count lives in device memory (qlist filled by an
     // earlier kernel); natural_rows: outputs go to the query's batch row
-    // perm[q] rather than to row qi of the list
+    // perm[q] rather than to row qi of the list; chunk: list entries per
+    // warp task
     if (nq_dev) n = *nq_dev;
     const int lane = threadIdx.x & 31;
     __shared__ int seeded_set[GF_KNN_BLOCK / 32][kSetSlots];
@@ -332,10 +333,10 @@ knn_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_t *__re
     unsigned long long ctr[5] = {0, 0, 0, 0, 0};
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t ntask = (n + kChunk - 1) / kChunk;
+    const int64_t ntask = (n + chunk - 1) / chunk;
     for (int64_t task = wid; task < ntask; task += nwarps) {
-        const int64_t q0 = task * kChunk;
-        const int64_t q1 = min(q0 + kChunk, n);
+        const int64_t q0 = task * chunk;
+        const int64_t q1 = min(q0 + (int64_t)chunk, n);
         int prev_h = -1, prev_ok = 0;
         ListState L;
         L.Ld = kInf;
@@ -1031,7 +1032,7 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
         // stays on the device; the grid strides over whatever it is)
         knn_kernel<false><<<148 * (2048 / GF_KNN_BLOCK), GF_KNN_BLOCK, 0, ctx->stream>>>(
             t.n, k, t.pos, t.perm, pos_batch, t.phalo, pstart, t.owner, t.knn, nearindex, dens, ctx->d_err,
-            nullptr, redo, nredo, true);
+            nullptr, redo, nredo, true, 1);  // scattered queries: one per warp task
         GF_LAUNCH_CHECK();
         return GF_OK;
     }
