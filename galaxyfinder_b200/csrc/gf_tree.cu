@@ -128,13 +128,17 @@ accum_mass(int64_t n, const float4 *__restrict__ pos, const int32_t *__restrict_
             }
         } else {
             const unsigned grp = __match_any_sync(0xffffffffu, node);
-            const double gw = group_sum(grp, w), gx = group_sum(grp, wx);
-            const double gy = group_sum(grp, wy), gz = group_sum(grp, wz);
-            if (node >= 0 && lane == __ffs(grp) - 1) {
-                atomicAdd(b.m + node, gw);
-                atomicAdd(b.mx + node, gx);
-                atomicAdd(b.my + node, gy);
-                atomicAdd(b.mz + node, gz);
+            // settled particles (node < 0) have nothing to add; their group
+            // skips the sums (the other groups shuffle within their own masks)
+            if (node >= 0) {
+                const double gw = group_sum(grp, w), gx = group_sum(grp, wx);
+                const double gy = group_sum(grp, wy), gz = group_sum(grp, wz);
+                if (lane == __ffs(grp) - 1) {
+                    atomicAdd(b.m + node, gw);
+                    atomicAdd(b.mx + node, gx);
+                    atomicAdd(b.my + node, gy);
+                    atomicAdd(b.mz + node, gz);
+                }
             }
         }
         __syncthreads();
@@ -160,6 +164,7 @@ accum_moments(int64_t n, const float4 *__restrict__ pos, const int32_t *__restri
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p - lane < n;
          p += (int64_t)gridDim.x * blockDim.x) {
         const int node = p < n ? pnode[p] : -1;
+        if (__all_sync(0xffffffffu, node < 0)) continue;  // a warp of settled particles
         float v[7] = {0, 0, 0, 0, 0, 0, 0};  // max |x - com|^2, then q0..q5
         unsigned bx[6] = {~0u, ~0u, ~0u, 0u, 0u, 0u};
         int key = 0;
@@ -206,7 +211,7 @@ accum_moments(int64_t n, const float4 *__restrict__ pos, const int32_t *__restri
             acc_r2 = 0.f;
             for (int i = 0; i < 6; i++) acc_q[i] = 0.f;
             for (int i = 0; i < 3; i++) { mn[i] = ~0u; mxk[i] = 0u; }
-            for (unsigned m = grp; m; m &= m - 1) {
+            for (unsigned m = node >= 0 ? grp : 0u; m; m &= m - 1) {  // settled lanes: nothing to gather
                 const int src = __ffs(m) - 1;
                 acc_r2 = fmaxf(acc_r2, __shfl_sync(grp, r2_self, src));
                 for (int i = 0; i < 6; i++) acc_q[i] += __shfl_sync(grp, q_self[i], src);
