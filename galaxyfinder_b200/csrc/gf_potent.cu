@@ -148,16 +148,19 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
 }
 
 // Per-halo total mass (FP64 sum of the float masses, as Self_Halo_Potent's
-// Mvir += mass[i]) and background term.
-__global__ void halo_bg_kernel(int32_t nhalo, const int64_t *__restrict__ pstart,
-                               const float4 *__restrict__ pos, PotentialParams pp,
-                               const int32_t *__restrict__ ntarget_halo,
-                               int32_t ndirect, double *__restrict__ bg,
-                               int32_t *__restrict__ direct) {
-    const int h = blockIdx.x;
+// Mvir += mass[i]) and background term.  Each halo's particles are summed in
+// kMassSplit slices by separate blocks (a large halo no longer holds one
+// block for its whole length), then the slices in order.
+constexpr int kMassSplit = 16;
+
+__global__ void halo_mass_kernel(int32_t nhalo, const int64_t *__restrict__ pstart,
+                                 const float4 *__restrict__ pos, double *__restrict__ part) {
+    const int h = blockIdx.x / kMassSplit, sl = blockIdx.x % kMassSplit;
     if (h >= nhalo) return;
+    const int64_t a0 = pstart[h], len = pstart[h + 1] - a0;
+    const int64_t a = a0 + len * sl / kMassSplit, b = a0 + len * (sl + 1) / kMassSplit;
     double s = 0.0;
-    for (int64_t p = pstart[h] + threadIdx.x; p < pstart[h + 1]; p += blockDim.x) s += (double)pos[p].w;
+    for (int64_t p = a + threadIdx.x; p < b; p += blockDim.x) s += (double)pos[p].w;
     __shared__ double red[256];
     red[threadIdx.x] = s;
     __syncthreads();
@@ -165,11 +168,38 @@ __global__ void halo_bg_kernel(int32_t nhalo, const int64_t *__restrict__ pstart
         if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        bg[h] = pp.add_bg ? bg_potent_dev(red[0], pp) : 0.0;
-        const int64_t nt = ntarget_halo ? ntarget_halo[h] : pstart[h + 1] - pstart[h];
-        direct[h] = nt < ndirect ? 1 : 0;
-    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void halo_bg_kernel(int32_t nhalo, const int64_t *__restrict__ pstart,
+                               const double *__restrict__ part, PotentialParams pp,
+                               const int32_t *__restrict__ ntarget_halo,
+                               int32_t ndirect, double *__restrict__ bg,
+                               int32_t *__restrict__ direct) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nhalo) return;
+    double m = 0.0;
+    for (int sl = 0; sl < kMassSplit; sl++) m += part[(int64_t)h * kMassSplit + sl];
+    bg[h] = pp.add_bg ? bg_potent_dev(m, pp) : 0.0;
+    const int64_t nt = ntarget_halo ? ntarget_halo[h] : pstart[h + 1] - pstart[h];
+    direct[h] = nt < ndirect ? 1 : 0;
+}
+
+// bg and direct flags of every halo of t (scratch in ctx->tmp[5]).
+int launch_halo_bg(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const PotentialParams &pp,
+                   const int32_t *ntarget_halo, double **bg, int32_t **direct) {
+    const size_t nb = (size_t)t.nhalo * sizeof(double);
+    const size_t np_ = (size_t)t.nhalo * kMassSplit * sizeof(double);
+    GF_TRY(ctx->tmp[5].reserve(nb + np_ + (size_t)t.nhalo * sizeof(int32_t) + 512));
+    *bg = ctx->tmp[5].as<double>();
+    double *part = *bg + t.nhalo;
+    *direct = reinterpret_cast<int32_t *>(part + (size_t)t.nhalo * kMassSplit);
+    halo_mass_kernel<<<t.nhalo * kMassSplit, 256, 0, ctx->stream>>>(t.nhalo, pstart, t.pos, part);
+    GF_LAUNCH_CHECK();
+    halo_bg_kernel<<<(t.nhalo + 127) / 128, 128, 0, ctx->stream>>>(t.nhalo, pstart, part, pp, ntarget_halo,
+                                                                   pp.ndirect, *bg, *direct);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
 }
 
 }  // namespace
@@ -180,13 +210,10 @@ int launch_self_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart,
                           const PotentialParams &pp, float *penergy, float *raw,
                           unsigned long long *counters) {
     if (t.n <= 0) return GF_OK;
-    GF_TRY(ctx->tmp[5].reserve(((size_t)t.nhalo * (sizeof(double) + sizeof(int32_t))) + 512));
-    double *bg = ctx->tmp[5].as<double>();
-    int32_t *direct = reinterpret_cast<int32_t *>(bg + t.nhalo);
     // tree-ordered positions carry the masses; halo h is still [pstart[h], pstart[h+1])
-    halo_bg_kernel<<<t.nhalo, 256, 0, ctx->stream>>>(t.nhalo, pstart, t.pos, pp, nullptr,
-                                                     pp.ndirect, bg, direct);
-    GF_LAUNCH_CHECK();
+    double *bg;
+    int32_t *direct;
+    GF_TRY(launch_halo_bg(ctx, t, pstart, pp, nullptr, &bg, &direct));
     const int block = GF_BH_BLOCK;
     int64_t grid = (t.n + block - 1) / block;
     grid = std::min<int64_t>(grid, 148LL * (2048 / block));
@@ -203,12 +230,9 @@ int launch_external_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pst
                               const int32_t *ntarget_halo, const PotentialParams &pp,
                               float *penergy, float *raw) {
     if (ntarget <= 0) return GF_OK;
-    GF_TRY(ctx->tmp[5].reserve(((size_t)t.nhalo * (sizeof(double) + sizeof(int32_t))) + 512));
-    double *bg = ctx->tmp[5].as<double>();
-    int32_t *direct = reinterpret_cast<int32_t *>(bg + t.nhalo);
-    halo_bg_kernel<<<t.nhalo, 256, 0, ctx->stream>>>(t.nhalo, pstart_src, t.pos, pp, ntarget_halo,
-                                                     pp.ndirect, bg, direct);
-    GF_LAUNCH_CHECK();
+    double *bg;
+    int32_t *direct;
+    GF_TRY(launch_halo_bg(ctx, t, pstart_src, pp, ntarget_halo, &bg, &direct));
     const int block = GF_BH_BLOCK;
     int64_t grid = std::min<int64_t>((ntarget + block - 1) / block, 148LL * (2048 / block));
     bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, nullptr, t.pos, t.root,
