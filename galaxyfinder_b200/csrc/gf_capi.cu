@@ -303,7 +303,8 @@ int gf_tuning_value(const char *name, int64_t *value) {
         const char *name;
         int64_t value;
     } params[] = {{"GF_KNN_ALGO", GF_KNN_ALGO},       {"GF_KNNB_BLOCK", GF_KNNB_BLOCK},
-                  {"GF_KNNB_ARITY", GF_KNNB_ARITY},   {"GF_KNN_BLOCK", GF_KNN_BLOCK},
+                  {"GF_KNNB_ARITY", GF_KNNB_ARITY},   {"GF_KNNB_SEEDS", GF_KNNB_SEEDS},
+                  {"GF_KNN_BLOCK", GF_KNN_BLOCK},
                   {"GF_KNN_MINB", GF_KNN_MINB},       {"GF_KNN_CHUNK", GF_KNN_CHUNK},
                   {"GF_BH_BLOCK", GF_BH_BLOCK},       {"GF_BH_MINB", GF_BH_MINB},
                   {"GF_FFT_PENCILS", GF_FFT_PENCILS}, {"GF_TREE_BLOCK", GF_TREE_BLOCK}};

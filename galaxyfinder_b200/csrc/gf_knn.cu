@@ -816,9 +816,9 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
             const int64_t hs = pstart[hl];
             const int64_t he = pstart[hl + 1];
             const int kk = (int)min((int64_t)k, he - hs);
-            // ---- seeds: the query's min(32, halo size) tree-order neighbours
-            const int ns = (int)min((int64_t)32, he - hs);
-            int64_t sw = q - 16;
+            // ---- seeds: the query's min(GF_KNNB_SEEDS, halo size) tree-order neighbours
+            const int ns = (int)min((int64_t)GF_KNNB_SEEDS, he - hs);
+            int64_t sw = q - GF_KNNB_SEEDS / 2;
             if (sw + ns > he) sw = he - ns;
             if (sw < hs) sw = hs;
             const int sw0 = (int)sw, sw1 = (int)sw + ns;

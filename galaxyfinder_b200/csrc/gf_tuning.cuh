@@ -22,6 +22,9 @@
 #ifndef GF_KNNB_MINB
 #define GF_KNNB_MINB 1
 #endif
+#ifndef GF_KNNB_SEEDS  // tree-order neighbours that seed each query's heap (float-key kernel)
+#define GF_KNNB_SEEDS 64
+#endif
 #ifndef GF_KNNB_ARITY  // children per node of the bucket kernel's per-lane heaps (2 or 4)
 #define GF_KNNB_ARITY 2
 #endif
@@ -43,6 +46,7 @@ static_assert(GF_KNN_CHUNK >= 1, "GF_KNN_CHUNK");
 static_assert(GF_KNNB_BLOCK % 32 == 0 && GF_KNNB_BLOCK <= 512, "GF_KNNB_BLOCK");
 static_assert(GF_KNN_ALGO >= 0 && GF_KNN_ALGO <= 2, "GF_KNN_ALGO");
 static_assert(GF_KNNB_ARITY == 2 || GF_KNNB_ARITY == 4, "GF_KNNB_ARITY");
+static_assert(GF_KNNB_SEEDS >= 32 && GF_KNNB_SEEDS % 2 == 0, "GF_KNNB_SEEDS");
 static_assert(GF_BH_BLOCK % 32 == 0 && GF_BH_BLOCK <= 1024, "GF_BH_BLOCK");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");
 static_assert(GF_TREE_BLOCK % 32 == 0 && GF_TREE_BLOCK >= 128 && GF_TREE_BLOCK <= 1024, "GF_TREE_BLOCK");

@@ -50,7 +50,7 @@ int gf_set_device(int device);
  * must prove the GPU path ran). */
 uint64_t gf_kernel_launch_count(void);
 /* Compile-time launch parameter `name` of this build (GF_KNN_ALGO,
- * GF_KNNB_BLOCK, GF_KNNB_ARITY, GF_KNN_BLOCK, GF_KNN_MINB, GF_KNN_CHUNK,
+ * GF_KNNB_BLOCK, GF_KNNB_ARITY, GF_KNNB_SEEDS, GF_KNN_BLOCK, GF_KNN_MINB, GF_KNN_CHUNK,
  * GF_BH_BLOCK, GF_BH_MINB, GF_FFT_PENCILS, GF_TREE_BLOCK) in *value.
  * Returns GF_EINVAL for an unknown name. */
 int gf_tuning_value(const char *name, int64_t *value);
