@@ -44,7 +44,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per particle of
 # each phase's dominant kernel, from one ncu capture of the 256-halo catalogue
 # (201,933 particles); the traffic scales with the particles processed.
-TRAFFIC_PER_PARTICLE = {"knn": (9.437952e6 + 1.28e3) / 201933}
+TRAFFIC_PER_PARTICLE = {"knn": (9.436672e6 + 1.536e3) / 201933}
 
 
 def parse():
