@@ -352,6 +352,61 @@ class Reference:
         return r, p2
 
 
+class ReferenceIO:
+    """The reference's FoF reader (FREAD) and GALFIND writer helpers
+    (GetHaloInfo, GetSubHaloInfo) from gfind.c, in oracle/_ref/libgfref_io.so
+    (loaded lazily: gfind.c's MPI calls stay unresolved and are never made)."""
+    _lib = None
+
+    def __init__(self, arena_mb: int = 512):
+        if ReferenceIO._lib is None:
+            path = REF_DIR / "libgfref_io.so"
+            if not path.exists():
+                if REF_SOURCE.exists():
+                    build(ref=True)
+                else:
+                    raise FileNotFoundError(f"{path} was not built (reference tree absent)")
+            import os
+            L = ctypes.CDLL(str(path), mode=os.RTLD_LAZY | os.RTLD_LOCAL)
+            L.io_init.argtypes = [ctypes.c_longlong]
+            L.io_layout.argtypes = [_VP]
+            L.io_fread.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_longlong, _F] + [_VP] * 9 + \
+                [ctypes.c_longlong]
+            L.io_fread.restype = ctypes.c_longlong
+            L.io_write_halo.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_longlong, _F, _I, _VP, _VP,
+                                        ctypes.c_longlong]
+            L.io_write_halo.restype = ctypes.c_longlong
+            if L.io_init(arena_mb) != 0:
+                raise RuntimeError("reference arena allocation failed")
+            ReferenceIO._lib = L
+        self.L = ReferenceIO._lib
+
+    def layout(self):
+        out = np.zeros(64, np.int64)
+        k = self.L.io_layout(_p(out))
+        return out[:k]
+
+    def fread(self, cat, mem, index, omep, cap):
+        o = {k: np.zeros(cap, np.float64) for k in ("x", "y", "z", "vx", "vy", "vz", "mass")}
+        t = np.zeros(cap, np.int32)
+        l02 = np.zeros(cap, np.float32)
+        n = self.L.io_fread(str(cat).encode(), str(mem).encode(), index, omep, _p(t), _p(o["x"]), _p(o["y"]),
+                            _p(o["z"]), _p(o["vx"]), _p(o["vy"]), _p(o["vz"]), _p(o["mass"]), _p(l02), cap)
+        if n < 0:
+            raise RuntimeError("io_fread failed")
+        o = {k: v[:n] for k, v in o.items()}
+        o["type"], o["link02"] = t[:n], l02[:n]
+        return o
+
+    def write_halo(self, cat, mem, index, omep, nsub, membership, cap=1 << 26):
+        buf = np.zeros(cap, np.uint8)
+        m = np.ascontiguousarray(membership, np.int64)
+        n = self.L.io_write_halo(str(cat).encode(), str(mem).encode(), index, omep, nsub, _p(m), _p(buf), cap)
+        if n < 0:
+            raise RuntimeError("io_write_halo failed")
+        return buf[:n].tobytes()
+
+
 class GalCenterSearch:
     """GalCenter's own centre search (find_centers.c:25-175), from
     oracle/_ref/libgalcenter.so."""
