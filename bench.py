@@ -118,8 +118,8 @@ class Clocks:
 # ------------------------------------------------------------------ reference (CPU)
 def reference_sample(hb, budget_s: float, seed: int = 7):
     """Halos of the catalogue in a seeded random order until the estimated
-    reference CPU time (~2e4 kNN queries/s/8 cores, survey probe) fills the
-    budget; always at least one halo."""
+    reference CPU time (about 2e4 kNN queries/s on 8 cores, measured on the
+    reference's findsphdensity) fills the budget; always at least one halo."""
     import oracle.oracle as orc
     rng = np.random.default_rng(seed)
     order = rng.permutation(hb.nhalo)
@@ -389,7 +389,11 @@ def main():
     dom = max(phases, key=phases.get)
     n = hb.n
     cells = st["mesh_cells"]
-    # algorithmic bytes per launch of each phase
+    # algorithmic bytes per launch of each phase: recentre reads FP64 x, y, z,
+    # m and writes FP64 x, y, z + float4 (52 B); kNN reads a float4 and
+    # writes k int32 indices and a float density; TSC reads FP64 x, y, z, m
+    # and writes the mesh once; smoothing reads and writes the mesh twice
+    # (16 B per cell floor); findDen reads FP64 x, y, z, the mesh, writes a float
     alg = {"recentre": 52 * n, "tree": 0, "knn": (16 + 4 * K_NEIGH + 4) * n,
            "tsc": 32 * n + 4 * cells, "smooth": 16 * cells, "findden": 28 * n + 4 * cells,
            "potential": 0}
