@@ -6,7 +6,8 @@
  *
  *  1. Drop-in entry points with the reference's exact C signatures.  A
  *     reference build links libgf's objects in place of its own definitions
- *      and the calls from subhalo_den() land here.  They take
+ *     (the reference objects with these symbols weakened, linked with the
+ *     whole libgf.a archive) and the calls from subhalo_den() land here.  They take
  *     the reference's host buffers, copy them to the GPU, run the kernels and
  *     copy results back before returning, so no host pointer is kept across
  *     calls (the reference's Memory2.c arena may move blocks between calls,
@@ -49,7 +50,7 @@ int gf_set_device(int device);
 /* Number of kernels this process has launched through libgf (for tests that
  * must prove the GPU path ran). */
 uint64_t gf_kernel_launch_count(void);
-/* Compile-time launch parameter `name` of this build (GF_KNN_ALGO,
+/* Compile-time launch parameter `name` of the loaded library (GF_KNN_ALGO,
  * GF_KNNB_BLOCK, GF_KNNB_ARITY, GF_KNNB_SEEDS, GF_KNN_BLOCK, GF_KNN_MINB, GF_KNN_CHUNK,
  * GF_BH_BLOCK, GF_BH_MINB, GF_FFT_PENCILS, GF_TREE_BLOCK) in *value.
  * Returns GF_EINVAL for an unknown name. */

@@ -6,8 +6,9 @@
 * ``Reference`` — oracle/_ref/libgfref_{fixed,asbuilt}.so, the reference's own
   NewGalFinder C compiled from its sources by oracle/Makefile, behind the thin
   harness in oracle/ref/ref_harness.c; ``Reference("linked")`` is the same
-  reference code with libgf's drop-ins linked in its place (the link recipe
-  of INTEGRATION.md), used to test the drop-in boundary inside the
+  reference code with libgf's drop-ins linked in its place (the reference
+  objects with the drop-in symbols weakened, linked with the whole libgf.a
+  archive; `make -C oracle linked`), used to test the drop-in boundary inside the
   reference's own pipeline.
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use this.

@@ -2,7 +2,8 @@
 
 oracle/_ref/libgfref_linked.so is the reference's NewGalFinder objects with
 the drop-in symbols weakened and libgf's objects linked in their place (the
-link recipe of INTEGRATION.md), so every call the reference makes to
+whole libgf.a archive over the weakened objects, `make -C oracle linked`),
+so every call the reference makes to
 lagFindStellarCore, findsphdensity, Self/External_Halo_Potent,
 CheckSelfTE/CheckExternalTE, the TSC/smoothing/findDen routines and
 i_potent_spline lands on the GPU, while MergingPeak, the watershed, the
