@@ -892,14 +892,24 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                         // filter: a branch-free pass over the tile against
                         // the bound at its start (the bound only tightens)
                         unsigned pass = 0;
+                        if (me && (base >= sw1 || base + m <= sw0)) {  // none of this lane's seeds here
 #pragma unroll 4
-                        for (int t = 0; t < m; t++) {
-                            const float f = f_d2_fma(Q, cpos[t]);
-                            const int p = base + t;
-                            const bool seed = p >= sw0 && p < sw1;
-                            const bool ok = me && !seed && f <= bf;
-                            pass |= (unsigned)ok << t;
-                            frej = (ok || seed || !me) ? frej : fminf(frej, f);
+                            for (int t = 0; t < m; t++) {
+                                const float f = f_d2_fma(Q, cpos[t]);
+                                const bool ok = f <= bf;
+                                pass |= (unsigned)ok << t;
+                                frej = ok ? frej : fminf(frej, f);
+                            }
+                        } else if (me) {
+#pragma unroll 4
+                            for (int t = 0; t < m; t++) {
+                                const float f = f_d2_fma(Q, cpos[t]);
+                                const int p = base + t;
+                                const bool seed = p >= sw0 && p < sw1;
+                                const bool ok = !seed && f <= bf;
+                                pass |= (unsigned)ok << t;
+                                frej = (ok || seed) ? frej : fminf(frej, f);
+                            }
                         }
                         if (COUNT) {
                             ctr[3] += __reduce_max_sync(0xffffffffu, (unsigned)__popc(pass));
