@@ -144,7 +144,8 @@ int compute_hid(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart, in
 // Mesh helpers implemented in gf_smooth.cu / gf_tsc.cu.
 int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
                        const double *mass, const int32_t *type, const int32_t *hid,
-                       const gf_mesh_desc *mesh, float *den, double volfact);
+                       const gf_mesh_desc *mesh, float *den, double volfact,
+                       const int32_t *order = nullptr);
 int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
                     const int32_t *hid, const gf_mesh_desc *mesh, const float *den, float *densph);
 int launch_scale(gf_ctx *ctx, float *den, int64_t ncells, double factor);

@@ -45,9 +45,13 @@ __global__ void tsc_deposit_kernel(int64_t n, const double *__restrict__ x,
                                    const int32_t *__restrict__ type,
                                    const int32_t *__restrict__ hid,
                                    const gf_mesh_desc *__restrict__ mesh,
-                                   float *__restrict__ den, float volfold, int *err) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
-         p += (int64_t)gridDim.x * blockDim.x) {
+                                   float *__restrict__ den, float volfold, int *err,
+                                   const int32_t *__restrict__ order) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        // with an order (the octree's permutation) a warp deposits spatial
+        // neighbours, whose stencils share cache lines of the mesh
+        const int64_t p = order ? (int64_t)order[t] : t;
         const gf_mesh_desc m = mesh[hid ? hid[p] : 0];
         if (m.ptype != GF_TYPE_ALL && (type ? type[p] : GF_TYPE_DM) != m.ptype) continue;
         Stencil s;
@@ -174,7 +178,7 @@ double tsc_volfact() {
 int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y,
                        const double *z, const double *mass, const int32_t *type,
                        const int32_t *hid, const gf_mesh_desc *mesh, float *den,
-                       double volfact) {
+                       double volfact, const int32_t *order) {
     if (n <= 0) return GF_OK;
     // A power-of-two volfact commutes with every float rounding, so folding
     // it into the weights gives the same bits as the reference's final
@@ -182,7 +186,7 @@ int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y,
     float fold = is_pow2_double(volfact) ? (float)volfact : 1.f;
     const int block = 256;
     tsc_deposit_kernel<<<grid_for(n, block), block, 0, ctx->stream>>>(
-        n, x, y, z, mass, type, hid, mesh, den, fold, ctx->d_err);
+        n, x, y, z, mass, type, hid, mesh, den, fold, ctx->d_err, order);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }
