@@ -147,7 +147,8 @@ int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y,
                        const gf_mesh_desc *mesh, float *den, double volfact,
                        const int32_t *order = nullptr);
 int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
-                    const int32_t *hid, const gf_mesh_desc *mesh, const float *den, float *densph);
+                    const int32_t *hid, const gf_mesh_desc *mesh, const float *den, float *densph,
+                    const int32_t *order = nullptr);
 int launch_scale(gf_ctx *ctx, float *den, int64_t ncells, double factor);
 int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
                   const gf_mesh_desc *mesh_dev, float *den);

@@ -202,7 +202,9 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         tm.mark();  // 4
         GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den));
         tm.mark();  // 5
-        if (o->dens_mesh) GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh));
+        if (o->dens_mesh)
+            GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh,
+                                   need_tree ? ctx->last_tree.perm : nullptr));
         tm.mark();  // 6
     } else {
         tm.mark();

@@ -102,9 +102,10 @@ __global__ void find_den_kernel(int64_t n, const double *__restrict__ x,
                                 const int32_t *__restrict__ hid,
                                 const gf_mesh_desc *__restrict__ mesh,
                                 const float *__restrict__ den, float *__restrict__ densph,
-                                int *err) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
-         p += (int64_t)gridDim.x * blockDim.x) {
+                                int *err, const int32_t *__restrict__ order) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = order ? (int64_t)order[t] : t;  // octree order: shared stencil lines
         const gf_mesh_desc m = mesh[hid ? hid[p] : 0];
         Stencil s;
         float xd1, yd1, zd1;
@@ -200,11 +201,11 @@ int launch_scale(gf_ctx *ctx, float *den, int64_t ncells, double factor) {
 
 int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
                     const int32_t *hid, const gf_mesh_desc *mesh, const float *den,
-                    float *densph) {
+                    float *densph, const int32_t *order) {
     if (n <= 0) return GF_OK;
     const int block = 256;
     find_den_kernel<<<grid_for(n, block), block, 0, ctx->stream>>>(n, x, y, z, hid, mesh, den,
-                                                                   densph, ctx->d_err);
+                                                                   densph, ctx->d_err, order);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }
