@@ -196,8 +196,10 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         float *den = ctx->tmp[3].as<float>();
         GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * cells, s));
         const double vf = tsc_volfact();
-        GF_TRY(launch_tsc_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, mesh_dev, den, vf,
-                                  need_tree ? ctx->last_tree.perm : nullptr));
+        // batch order: the deposit's float sums in octree order were faster
+        // (2.73 -> 2.34 ms) but put the densest cells of the 5e7-particle
+        // cluster 1.04e-5 from an FP64 deposit, past the 1e-5 target
+        GF_TRY(launch_tsc_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, mesh_dev, den, vf));
         if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, cells, vf));
         tm.mark();  // 4
         GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den));
