@@ -248,6 +248,17 @@ def core_density(ctx: Context, den, neighbor, type_, mass, peak):
     return out
 
 
+def chunk_cuts(pstart, nchunk: int) -> list[int]:
+    """Halo indices that split a batch into at most nchunk contiguous chunks
+    of similar particle counts: the first halo starting at or after each
+    multiple of n/nchunk particles (a halo larger than a chunk stays whole,
+    so there may be fewer chunks); ascending, from 0 to nhalo."""
+    ps = np.asarray(pstart, np.int64)
+    n = int(ps[-1])
+    cuts = [0] + [int(np.searchsorted(ps, c * n / nchunk)) for c in range(1, nchunk)] + [len(ps) - 1]
+    return sorted(set(cuts))
+
+
 class PipelinedStage:
     """The stage over a catalogue split into halo chunks of similar particle
     counts, each with its own context, CUDA stream, device buffers and host
@@ -273,13 +284,7 @@ class PipelinedStage:
         self.k = k
         dev = torch.device("cuda", device)
         ps = np.asarray(hb.pstart, np.int64)
-        n = int(ps[-1])
-        # halo boundaries closest to equal particle counts
-        cuts = [0]
-        for c in range(1, nchunk):
-            cuts.append(int(np.searchsorted(ps, c * n / nchunk)))
-        cuts.append(len(ps) - 1)
-        cuts = sorted(set(cuts))
+        cuts = chunk_cuts(ps, nchunk)
         self.chunks = []
         _, top = torch.cuda.Stream.priority_range()  # (least, greatest): (0, -3)
         for a, b in zip(cuts[:-1], cuts[1:]):
