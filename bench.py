@@ -45,6 +45,10 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # each phase's dominant kernel, from one ncu capture of the 256-halo catalogue
 # (201,933 particles); the traffic scales with the particles processed.
 TRAFFIC_PER_PARTICLE = {"knn": (9.436672e6 + 1.536e3) / 201933}
+# What bounds the kNN kernel instead of HBM, from the same capture: the tree
+# walk is latency- and issue-bound (its HBM traffic is a few bytes per query).
+KNN_LIMITER = ("latency/issue: 58.8% of issue slots active, 24.9% of warp slots occupied (shared-memory "
+               "heaps limit residency to 20 warps/SM), dominant stall 'wait'; DRAM 0.12% of peak")
 
 
 def parse():
@@ -406,6 +410,8 @@ def main():
                     "traffic": None if traffic is None else traffic * n,
                     "traffic_note": "bytes per launch, ncu capture of the 256-halo catalogue scaled by particles",
                     "algorithmic_bytes": alg[dom], "peak_source": pk["source"]}
+        if dom == "knn":
+            roofline["limiter"] = KNN_LIMITER
     else:
         # dominant phase has no HBM-bound roofline (tree build / FP32 potential walk);
         # report the largest HBM-bound phase instead
