@@ -42,3 +42,15 @@ def test_tuned_params_become_flags(tmp_path, monkeypatch):
     assert "-DGF_KNN_CHUNK=16" in flags and "-DGF_BH_BLOCK=64" in flags and "--fmad=false" in flags
     assert B.tuned_params() == {"GF_KNN_CHUNK": 16, "GF_BH_BLOCK": 64}
     assert T.variant_name({"GF_KNN_CHUNK": 16}) == "knn_chunk16"
+
+
+def test_library_reports_its_launch_parameters():
+    """gf_tuning_value reports the parameters the loaded library was compiled
+    with; build.py compiles with tuned.json's values."""
+    from galaxyfinder_b200 import _lib
+    params = B.tuned_params()
+    for name in ("GF_KNN_ALGO", "GF_KNNB_BLOCK", "GF_KNNB_SEEDS", "GF_BH_BLOCK", "GF_FFT_PENCILS"):
+        assert _lib.tuning_value(name) == params.get(name, T.DEFAULTS[name]), name
+    import pytest
+    with pytest.raises(_lib.GFError):
+        _lib.tuning_value("GF_NO_SUCH_PARAMETER")
