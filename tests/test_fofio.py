@@ -134,3 +134,31 @@ def test_writer_matches_reference(rio, files, tmp_path):
         lst = (tmp_path / "l").read_bytes()
         assert len(lst) == F.HALOINFO_DTYPE.itemsize + nsub * F.SUBINFO_DTYPE.itemsize
         assert lst[:F.HALOINFO_DTYPE.itemsize] == h0.tobytes()
+
+
+def test_empty_subhalo_and_single_kind_halo(rio, tmp_path):
+    """A halo of stars only, written with a sub-halo that has no member: the
+    reference divides its zero sums by a zero mass (NaN centre); so does the
+    writer."""
+    rng = np.random.default_rng(9)
+    halos = [_halo(rng, 0, 0, 0, 60)]
+    cat, mem = tmp_path / "cat", tmp_path / "mem"
+    F.write_catalogue(cat, mem, halos)
+    hb, _, _ = F.read_halos(cat, mem, OMEP)
+    assert hb.n == 60 and np.all(hb.type == F.TYPE_STAR)
+    memb = np.zeros(60, np.int64)  # every particle in sub-halo 0; sub-halo 1 empty
+    ref = rio.write_halo(cat, mem, 0, np.float32(OMEP), 2, memb)
+    with open(tmp_path / "d", "wb") as d, open(tmp_path / "b", "wb") as bg:
+        F.write_halo(halos[0], memb, 2, d, None, bg)
+    ours = (tmp_path / "d").read_bytes() + (tmp_path / "b").read_bytes()
+    (h0, s0), (h1, s1) = _parse(ref, 2), _parse(ours, 2)
+    assert h0.tobytes() == h1.tobytes()
+    for (si0, _), (si1, _) in zip(s0, s1):
+        for f in si0.dtype.names:
+            a, b = si0[f], si1[f]
+            if np.issubdtype(a.dtype, np.floating):
+                np.testing.assert_array_equal(np.isnan(a), np.isnan(b), err_msg=f)
+                np.testing.assert_array_equal(a[~np.isnan(a)], b[~np.isnan(b)], err_msg=f)
+            else:
+                np.testing.assert_array_equal(a, b, err_msg=f)
+    assert np.isnan(s1[1][0]["x"][0]) and s1[1][0]["npall"][0] == 0
