@@ -42,3 +42,29 @@ def test_core_entry_points_reject_bad_arguments():
     assert L.gf_density_peaks(None, 10, 32, None, None, None, 2000.0, 10, None, ctypes.byref(n)) == _lib.GF_EINVAL
     assert L.gf_core_density(None, 10, 32, None, None, None, None, 1, None, None, None, None, None, None,
                              None) == _lib.GF_EINVAL
+
+
+@pytest.mark.parametrize("seed,n,nsub", [(31, 2500, 3), (32, 6000, 6)])
+def test_restatement_vs_reference_functions(seed, n, nsub):
+    """The restatement against the reference's own finddenpeak and
+    FindCoreDensity (compiled into the oracle) on more clustered halos, with
+    the stellar peaks as cores too."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    from make_golden import blob
+    from oracle.oracle import Reference
+    ref = Reference("fixed")
+    p = blob(seed, n, 0.02, nsub=nsub)
+    rng = np.random.default_rng(seed)
+    mass = 10 ** rng.uniform(6, 8, n)
+    typ = np.where(rng.random(n) < 0.3, 1, 2).astype(np.int32)
+    idx, den = ref.findsphdensity(p[:, 0], p[:, 1], p[:, 2], mass, 32)
+    for jflag in (0, 1):
+        pk, _ = ref.finddenpeak(den, idx, typ, p[:, 0], p[:, 1], p[:, 2], jflag)
+        np.testing.assert_array_equal(cores.density_peaks(den, idx, typ if jflag else None), pk)
+        want = ref.FindCoreDensity(den, idx, typ, mass, pk)
+        got = cores.core_density(den, idx, typ, mass, pk)
+        for f in ("coredensity", "nummem", "numstar", "haloid", "flag"):
+            np.testing.assert_array_equal(got[f], want[f], err_msg=f"{f} jflag={jflag}")
+        np.testing.assert_allclose(got["starmass"], want["starmass"], rtol=1e-6)
