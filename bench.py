@@ -401,6 +401,14 @@ def main():
     alg = {"recentre": 52 * n, "tree": 0, "knn": (16 + 4 * K_NEIGH + 4) * n,
            "tsc": 32 * n + 4 * cells, "smooth": 16 * cells, "findden": 28 * n + 4 * cells,
            "potential": 0}
+    # the whole stage's algorithmic bytes per step against HBM, for the
+    # batched (pipelined and single-stream) and plain paths
+    stage_bytes = float(sum(alg.values()))
+
+    def stage_frac(ms_step):
+        return {"achieved_gbs": stage_bytes / (ms_step / 1e3) / 1e9,
+                "frac": stage_bytes / (ms_step / 1e3) / 1e9 / pk["hbm_gbs"]}
+    plain["stage_roofline"] = stage_frac(plain_ms)
     roofline = None
     if alg.get(dom):
         achieved = alg[dom] / (phases[dom] / 1e3) / 1e9
@@ -457,6 +465,9 @@ def main():
                 "d2h_bytes_per_step": pipe_d2h, "ms_per_step": pipe_res["e2e"]["ms_per_step"],
                 "path": "PipelinedStage.run_e2e(K): pinned host inputs in, all outputs back to pinned host, "
                         "every pass; each chunk streams its K passes back to back"},
+        "stage_roofline": dict(stage_frac(pipe_res["resident"]["ms_per_step"]), bytes_per_step=stage_bytes,
+                               note="all phases' algorithmic bytes per step (tree and potential count none) "
+                                    "over the step time, of measured HBM peak"),
         "single_stream": {"value": value, "ms_per_step": ms, "gpu_launches": int(launches),
                           "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                                   "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
