@@ -61,8 +61,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunks", type=int, default=8,
                     help="halo chunks (streams) of the pipelined stage")
-    ap.add_argument("--cpu-budget", type=float, default=12.0,
-                    help="seconds of reference CPU work for the cpu_baseline sample")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the comparison of sampled halos with the oracle")
     return ap.parse_args()
 
 
@@ -120,45 +120,43 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ reference (CPU)
-def reference_sample(hb, budget_s: float, seed: int = 7):
-    """Halos of the catalogue in a seeded random order until the estimated
-    reference CPU time (about 2e4 kNN queries/s on 8 cores, measured on the
-    reference's findsphdensity) fills the budget; always at least one halo."""
-    import oracle.oracle as orc
-    rng = np.random.default_rng(seed)
-    order = rng.permutation(hb.nhalo)
-    rate = 2.5e3 * orc.cpu_threads()  # particles/s of the whole reference stage, rough
-    chosen, total = [], 0
-    for h in order:
-        n = int(hb.pstart[h + 1] - hb.pstart[h])
-        if chosen and total + n > budget_s * rate:
-            continue
-        chosen.append(int(h))
-        total += n
-        if total > budget_s * rate:
-            break
-    return chosen, total
+# Halo-size strata (log N_p bins over the catalogue's range [100, 2e6]).  A
+# CPU sample times halos from every stratum: up to STRATUM_BUDGET particles
+# per stratum per step, at least one halo.  Halos above MAX_TIMED particles
+# take the reference minutes each, so they are not timed; their stratum is
+# extrapolated with the per-particle rate of the largest timed stratum, which
+# overstates the reference's speed there (its kNN cost per particle grows
+# with the halo size).
+STRATA = (100, 316, 1000, 3162, 10_000, 31_623, 100_000, 316_228, 2_000_001)
+STRATUM_BUDGET = 20_000
+MAX_TIMED = 250_000
+MESH_KW = dict(mode=2, nmin=64, nmax=256, rg=2.0, rg_in_cells=True)  # POW2 rule, 64-256^3
 
 
-def run_reference_stage(ref, hb, halos, mesh_rule):
-    """The reference's own functions on each sampled halo: findsphdensity
-    (kNN + W4), assign_density_TSC + gaussian_Smoothing + findDen, and
-    Self_Halo_Potent.  Returns seconds."""
-    from galaxyfinder_b200 import batch
-    t0 = time.perf_counter()
-    for h in halos:
-        p, a, b = recentred_halo(hb, h)
-        m = hb.mass[a:b]
-        ref.findsphdensity(p[:, 0], p[:, 1], p[:, 2], m, min(K_NEIGH, b - a))
-        mesh, _ = batch.plan_meshes(p.max(0)[None, :], mesh_rule)
-        mm = mesh[0]
-        n3 = (int(mm["nx"]), int(mm["ny"]), int(mm["nz"]))
-        o, cell = float(mm["xmin"]), float(mm["cellsize"])
-        den = ref.assign_density_TSC(p[:, 0], p[:, 1], p[:, 2], m, hb.type[a:b], *n3, o, o, o, cell, 5)
-        den = ref.gaussian_Smoothing(den, *n3, cell, float(mm["rg"]))
-        ref.findDen(p[:, 0], p[:, 1], p[:, 2], den, *n3, o, o, o, cell)
-        ref.Self_Halo_Potent(p[:, 0], p[:, 1], p[:, 2], m.astype(np.float32))
-    return time.perf_counter() - t0
+def halo_counts(hb):
+    return np.diff(np.asarray(hb.pstart, np.int64))
+
+
+def strata_of(hb):
+    n = halo_counts(hb)
+    return [np.flatnonzero((n >= a) & (n < b)) for a, b in zip(STRATA[:-1], STRATA[1:])]
+
+
+def stratified_sample(hb, step: int, seed: int = 7):
+    """Per stratum, the halos one CPU step times (seeded by the step)."""
+    n = halo_counts(hb)
+    rng = np.random.default_rng(seed + 1000 * step)
+    out = []
+    for halos in strata_of(hb):
+        timed = halos[n[halos] <= MAX_TIMED]
+        pick, tot = [], 0
+        for h in rng.permutation(timed):
+            pick.append(int(h))
+            tot += int(n[h])
+            if tot >= STRATUM_BUDGET:
+                break
+        out.append(pick)
+    return out
 
 
 def recentred_halo(hb, h):
@@ -171,6 +169,98 @@ def recentred_halo(hb, h):
         if c.max() - c.min() > 50.0 and cs.max() - cs.min() < c.max() - c.min():
             p[:, ax] = cs
     return p - p.min(axis=0), a, b
+
+
+def reference_halo_seconds(ref, hb, h, workers: int) -> float:
+    """The reference's own functions on one halo, as subhalo_den drives them:
+    findsphdensity (kNN + W4), assign_density_TSC, gaussian_Smoothing (FFTW
+    unavailable: its FFTs timed with the scipy.fft stand-in), findDen and
+    Self_Halo_Potent.  The mesh plan is the numpy restatement, so no repo
+    library is loaded.  Returns seconds."""
+    from oracle import fftw_standin, plan as oplan
+    t0 = time.perf_counter()
+    p, a, b = recentred_halo(hb, h)
+    m = hb.mass[a:b]
+    ref.findsphdensity(p[:, 0], p[:, 1], p[:, 2], m, min(K_NEIGH, b - a))
+    mm = oplan.plan_one(p.max(0), **MESH_KW)
+    n3 = (mm["nx"], mm["ny"], mm["nz"])
+    o, cell = mm["xmin"], mm["cellsize"]
+    den = ref.assign_density_TSC(p[:, 0], p[:, 1], p[:, 2], m, hb.type[a:b], *n3, o, o, o, cell, 5)
+    fftw_standin.gaussian_smoothing(den, *n3, cell, mm["rg"], workers=workers)
+    ref.findDen(p[:, 0], p[:, 1], p[:, 2], den, *n3, o, o, o, cell)
+    ref.Self_Halo_Potent(p[:, 0], p[:, 1], p[:, 2], m.astype(np.float32))
+    return time.perf_counter() - t0
+
+
+def reference_step(ref, hb, step: int, workers: int) -> dict:
+    """One CPU step: the stratified sample timed halo by halo, and the time the
+    whole catalogue would take at each stratum's measured rate."""
+    n = halo_counts(hb)
+    sample = stratified_sample(hb, step)
+    parts, secs = [], []
+    for halos in sample:
+        parts.append(int(n[halos].sum()) if halos else 0)
+        secs.append(sum(reference_halo_seconds(ref, hb, h, workers) for h in halos))
+    rates = [p / t if t > 0 else None for p, t in zip(parts, secs)]
+    extrap, last = 0.0, None
+    for s, halos in enumerate(strata_of(hb)):
+        r = rates[s] if rates[s] is not None else last  # untimed: largest timed stratum's rate
+        last = r if r is not None else last
+        extrap += float(n[halos].sum()) / r
+    return {"seconds": float(sum(secs)), "particles": int(sum(parts)), "extrap_s": extrap,
+            "rates": rates, "halos": [len(x) for x in sample]}
+
+
+def reference_baseline(hb, steps: int, warmup: int) -> dict:
+    import oracle.oracle as orc
+    ref = orc.Reference("fixed")
+    cores = orc.cpu_threads()
+    n = halo_counts(hb)
+    small = [int(h) for h in np.argsort(n)[:2]]
+    for _ in range(max(warmup, 1)):  # first touch of the reference's arena
+        for h in small:
+            reference_halo_seconds(ref, hb, h, cores)
+    res = [reference_step(ref, hb, j, cores) for j in range(steps)]
+    extrap = float(np.mean([r["extrap_s"] for r in res]))
+    strata = []
+    for s, halos in enumerate(strata_of(hb)):
+        rs = [r["rates"][s] for r in res if r["rates"][s] is not None]
+        strata.append({"n_p": [STRATA[s], STRATA[s + 1] - 1], "halos": int(len(halos)),
+                       "particles": int(n[halos].sum()),
+                       "timed_halos_per_step": float(np.mean([r["halos"][s] for r in res])),
+                       "rate": float(np.mean(rs)) if rs else None})
+    return {"value": float(hb.n) / extrap, "cores": cores, "extrap_s": extrap,
+            "step_seconds": float(np.mean([r["seconds"] for r in res])),
+            "step_particles": float(np.mean([r["particles"] for r in res])), "strata": strata}
+
+
+def reference_sample_text(rb, hb) -> str:
+    return (f"stratified by halo size: {len(STRATA) - 1} log N_p strata over [100, 2e6]; each step times up "
+            f"to {STRATUM_BUDGET} particles (at least one halo) per stratum, halos of at most {MAX_TIMED} "
+            f"particles, on average {rb['step_particles']:.0f} particles in {rb['step_seconds']:.1f} s; "
+            f"the whole {hb.n}-particle catalogue's time is the sum of each stratum's particles over its "
+            f"measured rate ({rb['extrap_s']:.0f} s); the {sum(1 for h in halo_counts(hb) if h > MAX_TIMED)} "
+            f"halos above {MAX_TIMED} particles take the largest timed stratum's rate (which overstates "
+            f"the reference's speed on them). findsphdensity + assign_density_TSC + gaussian_Smoothing + "
+            f"findDen + Self_Halo_Potent; FFTW unavailable: the smoothing's FFTs run on scipy.fft "
+            f"(single precision, all host threads) as the stand-in")
+
+
+def reference_line(args, hb, base_cfg):
+    try:
+        rb = reference_baseline(hb, args.steps, args.warmup)
+    except Exception as e:  # reference libraries missing on this host
+        return {"impl": "reference", "unavailable": f"reference build missing: {e}"}
+    line = dict(base_cfg)
+    line.update({"impl": "reference", "value": rb["value"], "ms_per_step": rb["step_seconds"] * 1e3,
+                 "cpu_baseline": {"value": rb["value"], "unit": UNIT, "cores": rb["cores"],
+                                  "kind": "reference", "sample": reference_sample_text(rb, hb),
+                                  "strata": rb["strata"], "catalogue_seconds": rb["extrap_s"]},
+                 "e2e": {"value": rb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0},
+                 "note": "ms_per_step is the measured time of one step's stratified sample; value is the "
+                         "catalogue's particles over its time extrapolated stratum by stratum"})
+    return line
 
 
 def run_dropin_stage(hb, halos, mesh_rule):
@@ -204,27 +294,142 @@ def run_dropin_stage(hb, halos, mesh_rule):
     return time.perf_counter() - t0
 
 
-def reference_line(args, hb, mesh_rule, base_cfg):
-    import oracle.oracle as orc
-    try:
-        ref = orc.Reference("fixed")
-    except Exception as e:  # reference libraries missing on this host
-        return {"impl": "reference", "unavailable": f"reference build missing: {e}"}
-    halos, npart = reference_sample(hb, budget_s=3.0)
-    run_reference_stage(ref, hb, halos[:1], mesh_rule)  # warm-up: arena, page faults
-    times = [run_reference_stage(ref, hb, halos, mesh_rule) for _ in range(args.steps)]
-    t = sum(times) / len(times)
-    value = npart / t
-    cores = orc.cpu_threads()
-    sample = (f"{len(halos)} of {hb.nhalo} catalogue halos ({npart} particles), seeded random "
-              f"order; FFTW unavailable: gaussian_Smoothing runs on the FP64 fftw3f shim")
-    line = dict(base_cfg)
-    line.update({"impl": "reference", "value": value, "ms_per_step": t * 1e3,
-                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
-                                  "kind": "reference", "sample": sample},
-                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                         "d2h_bytes_per_step": 0}})
-    return line
+def catalogue_mesh_cells(hb) -> int:
+    """Mesh floats of the whole catalogue under the POW2 rule (numpy plan)."""
+    from oracle import plan as oplan
+    ext = np.array([recentred_halo(hb, h)[0].max(0) for h in range(hb.nhalo)])
+    return int(oplan.plan(ext, **MESH_KW)[1])
+
+
+def workload_config(args, hb, world: int, mesh_cells: int) -> dict:
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": f"batched catalogue, {args.nhalo} FoF halos per GPU, N_p ~ N^-1.9 on [100, 2e6], "
+                        "k=32, per-halo TSC mesh 64-256^3, Gaussian 2 cells, Barnes-Hut theta2=0.5",
+            "nhalo": args.nhalo, "particles_per_gpu": int(hb.n), "mesh_cells": int(mesh_cells),
+            "l2": "inputs and working set larger than L2 (no flush needed)",
+            "parallelism": f"halo shards x{world} (no collective on the data path)"}
+
+
+# ------------------------------------------------------------------ accuracy (oracle)
+def accuracy_sample(hb, per_stratum: int = 9, seed: int = 11):
+    """Halos of every size stratum (all of the largest), at least 64."""
+    rng = np.random.default_rng(seed)
+    pick = []
+    for halos in strata_of(hb):
+        pick += [int(h) for h in rng.permutation(halos)[:per_stratum]]
+    return sorted(pick)
+
+
+def accuracy_check(ctx, db, cfg, hb, mesh_rule, halos, rows_per_halo: int = 1500) -> dict:
+    """The stage's outputs on sampled halos against the oracle: kNN lists and
+    SPH densities against exact kNN (the C restatement, or for halos above
+    40k particles a k-d tree over all the halo's FP32 positions, re-ranked in
+    exact FP64 (d^2, index) order, on sampled rows); mesh density against the
+    FP64 chain (TSC in FP64, FP64 spectral smoothing, findDen); the raw tree
+    potential against an FP64 walk of the same tree on sampled particles."""
+    import scipy.fft as sf
+    import torch
+    from scipy.spatial import cKDTree
+
+    from galaxyfinder_b200 import _lib, batch
+    from oracle import adjoint as A
+    from oracle.oracle import Restatement
+
+    R = Restatement()
+    out = batch.StageBuffers(hb.n, K_NEIGH, db.x.device, keep_positions=True, keep_phi=True)
+    _, st = batch.stage_run(ctx, db, cfg, out, stats=True)
+    torch.cuda.synchronize()
+    nn = int(st["nnode"])
+    bh = np.zeros(nn, _lib.BH_NODE_DTYPE)
+    tpos = np.zeros((hb.n, 4), np.float32)
+    root = np.zeros(hb.nhalo, np.int32)
+    rend = np.zeros(hb.nhalo, np.int32)
+    _lib.check(_lib.lib().gf_tree_export(ctx.handle, _lib.ptr(bh), None, _lib.ptr(tpos), None,
+                                         _lib.ptr(root), _lib.ptr(rend)))
+    xr = np.stack([out.xr.cpu().numpy(), out.yr.cpu().numpy(), out.zr.cpu().numpy()], 1)
+    near = out.nearindex.cpu().numpy()
+    dsph = out.dens_sph.cpu().numpy()
+    dmesh = out.dens_mesh.cpu().numpy()
+    phi = out.phi.cpu().numpy().astype(np.float64)
+    rng = np.random.default_rng(5)
+    acc = {"halos": len(halos), "particles": 0, "knn_rows": 0, "knn_mismatch": 0, "sph_mismatch": 0,
+           "sph_rel_max": 0.0, "mesh_particles": 0, "mesh_rel_max_dense": 0.0, "mesh_above_1e-5": 0,
+           "mesh_rel": [], "pot_rows": 0, "potential_rel_max": 0.0, "pot_rel": []}
+    for h in halos:
+        a, b = int(hb.pstart[h]), int(hb.pstart[h + 1])
+        n = b - a
+        acc["particles"] += n
+        p = xr[a:b]
+        q = p.astype(np.float32)
+        k = min(K_NEIGH, n)
+        # kNN + SPH
+        if n <= 40_000:
+            rows = np.arange(n)
+            idx, d2 = R.knn(q[:, 0], q[:, 1], q[:, 2], k)
+        else:
+            rows = np.sort(rng.choice(n, rows_per_halo, replace=False))
+            q64 = q.astype(np.float64)
+            _, cand = cKDTree(q64).query(q64[rows], k=k + 16, workers=-1)
+            idx = np.zeros((len(rows), k), np.int64)
+            d2 = np.zeros((len(rows), k))
+            for r, i in enumerate(rows):
+                c = cand[r]
+                d = q64[c] - q64[i]
+                dd = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+                o = np.lexsort((c, dd))
+                idx[r], d2[r] = c[o[:k]], dd[o[:k]]
+        acc["knn_rows"] += len(rows)
+        acc["knn_mismatch"] += int(np.sum(np.any(near[a:b][rows, :k] != idx, axis=1)))
+        sph = R.sph_density(d2)
+        g = dsph[a:b][rows]
+        acc["sph_mismatch"] += int(np.sum(g != sph))
+        acc["sph_rel_max"] = max(acc["sph_rel_max"], float(np.max(np.abs(g.astype(np.float64) - sph) /
+                                                                  np.maximum(np.abs(sph), 1e-300))))
+        # mesh density: FP64 chain
+        mm, _ = batch.plan_meshes(p.max(0)[None, :], mesh_rule)
+        m = mm[0]
+        n3 = (int(m["nx"]), int(m["ny"]), int(m["nz"]))
+        o, cell = float(m["xmin"]), float(m["cellsize"])
+        den = R.tsc(p[:, 0], p[:, 1], p[:, 2], hb.mass[a:b], hb.type[a:b], *n3, o, o, o, cell, 5,
+                    acc_double=True)
+        mesh = A.Mesh.from_desc(m)
+        grid = np.asarray(den, np.float64).reshape(mesh.nz, mesh.ny, mesh.mx)[:, :, :mesh.nx]
+        s = sf.irfftn(sf.rfftn(grid, workers=-1) * A._filter(mesh), s=(mesh.nz, mesh.ny, mesh.nx),
+                      axes=(0, 1, 2), workers=-1)
+        full = mesh.zeros()
+        full[:, :, :mesh.nx] = s
+        ref = R.find_den(p[:, 0], p[:, 1], p[:, 2], full.ravel().astype(np.float32), *n3, o, o, o,
+                         cell).astype(np.float64)
+        got = dmesh[a:b].astype(np.float64)
+        pos = ref > 0
+        rel = np.abs(got[pos] - ref[pos]) / ref[pos]
+        dense = ref[pos] > 1e-3 * ref.max()
+        acc["mesh_particles"] += int(pos.sum())
+        acc["mesh_above_1e-5"] += int(np.sum(rel > 1e-5))
+        acc["mesh_rel_max_dense"] = max(acc["mesh_rel_max_dense"], float(rel[dense].max()))
+        acc["mesh_rel"].append(rel)
+        # potential: raw phi vs FP64 walk of the same tree
+        prow = np.arange(n) if n <= 2 * rows_per_halo else np.sort(rng.choice(n, rows_per_halo, replace=False))
+        topen = np.full(len(prow), int(n < 100), np.int32)  # Self_Halo_Potent's direct branch
+        f64 = R.tree_potential(bh, tpos, q[prow], np.full(len(prow), root[h], np.int32),
+                               np.full(len(prow), rend[h], np.int32), topen)
+        prel = np.abs(phi[a:b][prow] - f64) / np.abs(f64)
+        acc["pot_rows"] += len(prow)
+        acc["potential_rel_max"] = max(acc["potential_rel_max"], float(prel.max()))
+        acc["pot_rel"].append(prel)
+    mrel = np.concatenate(acc.pop("mesh_rel"))
+    prel = np.concatenate(acc.pop("pot_rel"))
+    acc["mesh_rel_p99"] = float(np.quantile(mrel, 0.99))
+    acc["mesh_rel_median"] = float(np.median(mrel))
+    acc["mesh_frac_above_1e-5"] = acc["mesh_above_1e-5"] / max(acc["mesh_particles"], 1)
+    acc["potential_rel_median"] = float(np.median(prel))
+    acc["largest_halo"] = int(max(halo_counts(hb)[halos]))
+    acc["bars"] = {"knn": "bit-exact", "sph": "bit-exact", "mesh": "1e-5 relative where rho > 1e-3 rho_max "
+                   "(below, the FP32 mesh's absolute roundoff)", "potential": "1e-6 relative (raw phi vs FP64 "
+                   "walk of the same tree)"}
+    acc["pass"] = bool(acc["knn_mismatch"] == 0 and acc["sph_mismatch"] == 0 and
+                       acc["mesh_rel_max_dense"] < 1e-5 and acc["potential_rel_max"] < 1e-6)
+    return acc
 
 
 # ------------------------------------------------------------------ main
@@ -254,10 +459,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             hb = synth.catalogue(seed=synth.SEED_BASE + 2, nhalo=args.nhalo)
-            line = reference_line(args, hb, mesh_rule, base)
+            line = reference_line(args, hb, base)
             line["n_gpus"] = world
-            line["config"] = {"workload": f"batched catalogue, {args.nhalo} FoF halos, N_p ~ N^-1.9 "
-                              "on [100, 2e6], k=32, per-halo TSC mesh 64-256^3, theta2=0.5"}
+            line["config"] = workload_config(args, hb, world, catalogue_mesh_cells(hb))
             print(json.dumps(line), flush=True)
         if dist is not None:
             dist.destroy_process_group()
@@ -398,8 +602,10 @@ def main():
     # writes k int32 indices and a float density; TSC reads FP64 x, y, z, m
     # and writes the mesh once; smoothing reads and writes the mesh twice
     # (16 B per cell floor); findDen reads FP64 x, y, z, the mesh, writes a float
+    # (its 27-cell stencils re-read the mesh the smoothing has just written,
+    # shared between neighbouring particles: working set, not counted)
     alg = {"recentre": 52 * n, "tree": 0, "knn": (16 + 4 * K_NEIGH + 4) * n,
-           "tsc": 32 * n + 4 * cells, "smooth": 16 * cells, "findden": 28 * n + 4 * cells,
+           "tsc": 32 * n + 4 * cells, "smooth": 16 * cells, "findden": 28 * n,
            "potential": 0}
     # the whole stage's algorithmic bytes per step against HBM, for the
     # batched (pipelined and single-stream) and plain paths
@@ -453,14 +659,9 @@ def main():
     line = dict(base)
     line.update({
         "value": pipe_res["resident"]["value"], "ms_per_step": pipe_res["resident"]["ms_per_step"],
-        "config": {"workload": f"batched catalogue, {args.nhalo} FoF halos per GPU, N_p ~ N^-1.9 on "
-                               f"[100, 2e6] ({hb.n} particles on rank 0), k=32, per-halo TSC mesh "
-                               "64-256^3, Gaussian 2 cells, Barnes-Hut theta2=0.5",
-                   "nhalo": args.nhalo, "particles_per_gpu": hb.n,
-                   "mesh_cells": int(cells), "tree_nodes": int(st["nnode"]),
-                   "l2": "inputs and working set larger than L2 (no flush needed)",
-                   "parallelism": f"halo shards x{world} (no collective on the data path)",
-                   "pipeline": f"{nchunks} halo chunks on their own streams and host threads"},
+        "config": workload_config(args, hb, world, int(cells)),
+        "pipeline": f"{nchunks} halo chunks on their own streams and host threads",
+        "tree_nodes": int(st["nnode"]),
         "e2e": {"value": pipe_res["e2e"]["value"], "unit": UNIT, "h2d_bytes_per_step": pipe_h2d,
                 "d2h_bytes_per_step": pipe_d2h, "ms_per_step": pipe_res["e2e"]["ms_per_step"],
                 "path": "PipelinedStage.run_e2e(K): pinned host inputs in, all outputs back to pinned host, "
@@ -482,28 +683,31 @@ def main():
         "clocks": clk,
     })
 
-    # ---- CPU baseline: the reference's own code on a bounded sample
+    # ---- CPU baseline (the reference's own code on a bounded stratified
+    # sample), the drop-in path on one step of that sample, and the stage's
+    # accuracy on sampled halos against the oracle
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            import oracle.oracle as orc
-            ref = orc.Reference("fixed")
-            halos, npart = reference_sample(hb, args.cpu_budget)
-            t = run_reference_stage(ref, hb, halos, mesh_rule)
+            rb = reference_baseline(hb, steps=1, warmup=1)
+            line["cpu_baseline"] = {"value": rb["value"], "unit": UNIT, "cores": rb["cores"],
+                                    "kind": "reference", "sample": reference_sample_text(rb, hb),
+                                    "strata": rb["strata"], "catalogue_seconds": rb["extrap_s"]}
+            halos = [h for s_ in stratified_sample(hb, 0) for h in s_]
+            npart = int(halo_counts(hb)[halos].sum())
             run_dropin_stage(hb, halos[:2], mesh_rule)
             td = run_dropin_stage(hb, halos, mesh_rule)
             line["plain"]["dropin"] = {
                 "value": npart / td, "unit": UNIT, "seconds": td,
                 "path": "reference signatures (findsphdensity, assign_density_TSC, "
                         "gaussian_Smoothing, findDen, Self_Halo_Potent), host buffers, "
-                        "one halo per call, on the cpu_baseline sample"}
-            line["cpu_baseline"] = {
-                "value": npart / t, "unit": UNIT, "cores": orc.cpu_threads(), "kind": "reference",
-                "sample": f"{len(halos)} of {hb.nhalo} halos ({npart} particles, seeded random order); "
-                          "findsphdensity + TSC/gaussian_Smoothing/findDen + Self_Halo_Potent; "
-                          "FFTW unavailable: FP64 fftw3f shim"}
+                        "one halo per call, on one step of the cpu_baseline sample "
+                        f"({len(halos)} halos, {npart} particles)"}
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                     "sample": f"unavailable: {e}"}
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        halos = accuracy_sample(hb)
+        line["accuracy"] = accuracy_check(ctx, db, cfg, hb, mesh_rule, halos)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

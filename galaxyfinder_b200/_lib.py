@@ -102,7 +102,7 @@ class StageOut(ctypes.Structure):
     _fields_ = [
         ("nearindex", ctypes.c_void_p), ("dens_sph", ctypes.c_void_p),
         ("dens_mesh", ctypes.c_void_p), ("penergy", ctypes.c_void_p), ("xr", ctypes.c_void_p),
-        ("yr", ctypes.c_void_p), ("zr", ctypes.c_void_p),
+        ("yr", ctypes.c_void_p), ("zr", ctypes.c_void_p), ("phi", ctypes.c_void_p),
     ]
 
 
@@ -193,6 +193,7 @@ SIGNATURES = {
     "gf_mesh_peaks": (_INT, [_VP, _I32, _VP, _VP, _VP, _INT, _F, _I64, _VP, _VP, _VP,
                              ctypes.POINTER(_I64)]),
     "gf_self_potential": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _I32, _D, _INT, _VP, _VP]),
+    "gf_bg_potent_device": (_INT, [_VP, _I32, _VP, _VP]),
     "gf_stage_run": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),
                             ctypes.POINTER(StageOut), ctypes.POINTER(StageStats)]),
 }

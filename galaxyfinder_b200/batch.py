@@ -157,11 +157,13 @@ def stage_config(mesh: MeshRule | None = None, box=100.0, knn_k=32, do_mesh=True
 class StageBuffers:
     """Device outputs of gf_stage_run for a batch of n particles."""
 
-    def __init__(self, n: int, k: int, device, keep_positions=False):
+    def __init__(self, n: int, k: int, device, keep_positions=False, keep_phi=False):
         self.nearindex = torch.empty((n, max(k, 1)), dtype=torch.int32, device=device)
         self.dens_sph = torch.empty(n, dtype=torch.float32, device=device)
         self.dens_mesh = torch.empty(n, dtype=torch.float32, device=device)
         self.penergy = torch.empty(n, dtype=torch.float32, device=device)
+        # raw tree potential phi (penergy = phi * potentfact + bg, rounded to float)
+        self.phi = torch.empty(n, dtype=torch.float32, device=device) if keep_phi else None
         self.xr = self.yr = self.zr = None
         if keep_positions:
             self.xr = torch.empty(n, dtype=torch.float64, device=device)
@@ -170,7 +172,7 @@ class StageBuffers:
 
     def c(self) -> _lib.StageOut:
         return _lib.StageOut(ptr(self.nearindex), ptr(self.dens_sph), ptr(self.dens_mesh),
-                             ptr(self.penergy), ptr(self.xr), ptr(self.yr), ptr(self.zr))
+                             ptr(self.penergy), ptr(self.xr), ptr(self.yr), ptr(self.zr), ptr(self.phi))
 
 
 class HaloViews:
@@ -191,7 +193,7 @@ class HaloViews:
                       batch.mass.data_ptr() + 8 * a, batch.type.data_ptr() + 4 * a)
             o = _lib.StageOut(out.nearindex.data_ptr() + 4 * kk * a, out.dens_sph.data_ptr() + 4 * a,
                               out.dens_mesh.data_ptr() + 4 * a, out.penergy.data_ptr() + 4 * a,
-                              None, None, None)
+                              None, None, None, None)
             self.views.append((b, o))
 
     def run(self, ctx: Context, cfg: _lib.StageConfig, halos=None):
@@ -205,7 +207,7 @@ def stage_run(ctx: Context, batch: DeviceBatch, cfg: _lib.StageConfig,
               out: StageBuffers | None = None, stats=False):
     """Runs the whole density-and-potential stage on the batch."""
     if out is None:
-        out = StageBuffers(batch.n, cfg.knn_k, batch.x.device, keep_positions=True)
+        out = StageBuffers(batch.n, cfg.knn_k, batch.x.device, keep_positions=True, keep_phi=True)
     st = _lib.StageStats() if stats else None
     b = batch.c()
     oc = out.c()

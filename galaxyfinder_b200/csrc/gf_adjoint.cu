@@ -24,7 +24,7 @@ namespace gf {
 namespace {
 
 int grid_for(int64_t n) {
-    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sm_count() * 16));
 }
 
 // dL/dm_p = volfact sum_c G[c] W_c,  dL/dx_p = volfact m_p sum_c G[c] dW_c/dx
@@ -317,7 +317,7 @@ int launch_mesh_peaks(gf_ctx *ctx, int32_t nhalo, int64_t maxcell, const gf_mesh
                       const float *den, int margin, float threshold, int64_t cap, int32_t *out_halo,
                       int64_t *out_cell, float *out_val, unsigned long long *dcount) {
     GF_CUDA_TRY(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), ctx->stream));
-    const int64_t gx = std::min<int64_t>((maxcell + 255) / 256, 148 * 8);
+    const int64_t gx = std::min<int64_t>((maxcell + 255) / 256, sm_count() * 8);
     dim3 grid((unsigned)std::max<int64_t>(gx, 1), (unsigned)nhalo);
     mesh_peaks_kernel<<<grid, 256, 0, ctx->stream>>>(mesh_dev, den, margin, threshold, cap, out_halo,
                                                     out_cell, out_val, dcount);
@@ -369,7 +369,7 @@ int gf_knn_density_adjoint(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t 
     }
     if (nq == 0 || n == 0) return GF_OK;
     std::lock_guard<std::mutex> g(ctx->lock);
-    const int64_t blocks = std::min<int64_t>((nq * 32 + 255) / 256, 148 * 16);
+    const int64_t blocks = std::min<int64_t>((nq * 32 + 255) / 256, sm_count() * 16);
     knn_density_adjoint_kernel<<<(int)std::max<int64_t>(blocks, 1), 256, 0, ctx->stream>>>(
         nq, qidx_dev, n, x, y, z, nhalo, pstart_dev, k, nearindex, gdens, gx, gy, gz, ctx->d_err);
     GF_LAUNCH_CHECK();

@@ -23,7 +23,7 @@ namespace gf {
 namespace {
 
 int grid_for(int64_t n) {
-    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sm_count() * 16));
 }
 
 // KE_i = 1/2 |(x_i - c) r1 + (v_i - v_c) r2|^2 (subhaloden.mod6.c:1787-1795,
@@ -418,7 +418,7 @@ int gf_tidal_radius(Coretype *core, int numcore, const int32_t *score_core, int 
             reinterpret_cast<double *>(d + o_d2), reinterpret_cast<float *>(d + o_mm));
         GF_LAUNCH_CHECK();
         const int warps_per_block = 8;
-        const int blocks = (int)std::min<int64_t>((npair + warps_per_block - 1) / warps_per_block, 148 * 32);
+        const int blocks = (int)std::min<int64_t>((npair + warps_per_block - 1) / warps_per_block, sm_count() * 32);
         enclosed_kernel<<<blocks, 32 * warps_per_block, 0, s>>>(
             npair, reinterpret_cast<const int32_t *>(d + o_pj), reinterpret_cast<const double *>(d + o_pr),
             reinterpret_cast<const int64_t *>(d + o_ms), reinterpret_cast<const double *>(d + o_d2),

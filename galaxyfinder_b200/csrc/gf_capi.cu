@@ -13,6 +13,22 @@ namespace gf {
 
 std::atomic<uint64_t> g_launches{0};
 
+int sm_count() {
+    constexpr int kMaxDev = 64;
+    static std::atomic<int> cache[kMaxDev];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) dev = -1;
+    if (dev >= 0) {
+        const int v = cache[dev].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+    }
+    int c = 0;
+    if (dev < 0 || cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0)
+        return 1;  // no usable device: the launch that follows reports the error
+    cache[dev].store(c, std::memory_order_relaxed);
+    return c;
+}
+
 namespace {
 thread_local int t_status = GF_OK;
 thread_local char t_msg[512] = "";
@@ -199,7 +215,7 @@ void ensure_physics() {
 
 int compute_hid(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart, int32_t *hid) {
     if (n <= 0) return GF_OK;
-    int64_t g = std::min<int64_t>((n + 255) / 256, 148 * 16);
+    int64_t g = std::min<int64_t>((n + 255) / 256, sm_count() * 16);
     hid_kernel<<<(int)g, 256, 0, ctx->stream>>>(nhalo, n, pstart, hid);
     GF_LAUNCH_CHECK();
     return GF_OK;

@@ -64,7 +64,7 @@ constexpr int kBisectMax = 200;               // the bisection halves its bracke
 constexpr int kCoreBlock = 256;
 
 int grid_for(int64_t n) {
-    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sm_count() * 16));
 }
 
 __global__ void peak_kernel(int np, int K, const float *__restrict__ den, const int32_t *__restrict__ nbr,
@@ -315,7 +315,7 @@ int core_density(gf_ctx *ctx, int32_t np, int K, const float *den, const int32_t
     // concurrent searches: one per block, each with its bitmap and queue,
     // within about 1 GiB of scratch
     const int64_t slot = words * 4 + (int64_t)np * 4;
-    const int64_t slots = std::max<int64_t>(1, std::min<int64_t>({(int64_t)ncore, (1LL << 30) / slot, 148 * 8}));
+    const int64_t slots = std::max<int64_t>(1, std::min<int64_t>({(int64_t)ncore, (1LL << 30) / slot, sm_count() * 8}));
     // scratch: [min density | peak flags | bitmaps | queues]
     const size_t head = 256, flags = ((size_t)np + 255) & ~size_t(255);
     GF_TRY(ctx->tmp[1].reserve(head + flags + (size_t)(slots * slot)));

@@ -50,7 +50,7 @@ constexpr float kPeakThreshold = 2000.f; // PEAKTHRESHOLD 2000.L, params.h:19 (e
 constexpr int kMergeAbove = 10;          // nnost.c:1289
 
 int grid_for(int64_t n) {
-    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sm_count() * 16));
 }
 
 __global__ void unit_pos_kernel(int64_t n, const double *__restrict__ x, const double *__restrict__ y,

@@ -20,6 +20,10 @@ void set_status(int status, const char *fmt, ...);
 void clear_status();
 int last_status();
 
+// Streaming multiprocessors of the current device (queried once per device);
+// grid-stride launches size their grids as a multiple of it.
+int sm_count();
+
 // Counts every kernel launch issued through libgf.
 extern std::atomic<uint64_t> g_launches;
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }

@@ -1034,13 +1034,13 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
         GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, shmem));
         const int64_t nbucket = (t.n + 31) / 32;
         int64_t grid = (nbucket * 32 + block - 1) / block;
-        grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * std::max(per_sm, 1)));
+        grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)sm_count() * std::max(per_sm, 1)));
         kern<<<(int)grid, block, shmem, ctx->stream>>>(t.n, k, t.pos, t.perm, pos_batch, t.phalo, pstart, t.owner,
                                                        t.knn, nearindex, dens, redo, nredo, counters);
         GF_LAUNCH_CHECK();
         // the uncertified queries, exactly, into their own rows (the count
         // stays on the device; the grid strides over whatever it is)
-        knn_kernel<false><<<148 * (2048 / GF_KNN_BLOCK), GF_KNN_BLOCK, 0, ctx->stream>>>(
+        knn_kernel<false><<<sm_count() * (2048 / GF_KNN_BLOCK), GF_KNN_BLOCK, 0, ctx->stream>>>(
             t.n, k, t.pos, t.perm, pos_batch, t.phalo, pstart, t.owner, t.knn, nearindex, dens, ctx->d_err,
             nullptr, redo, nredo, true, 1);  // scattered queries: one per warp task
         GF_LAUNCH_CHECK();
@@ -1055,7 +1055,7 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
         GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, shmem));
         const int64_t nbucket = (t.n + 31) / 32;
         int64_t grid = (nbucket * 32 + block - 1) / block;
-        grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * std::max(per_sm, 1)));
+        grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)sm_count() * std::max(per_sm, 1)));
         kern<<<(int)grid, block, shmem, ctx->stream>>>(t.n, k, t.pos, t.perm, t.phalo, pstart, t.owner, t.knn,
                                                        nearindex, dens, ctx->d_err, counters);
         GF_LAUNCH_CHECK();
@@ -1064,7 +1064,7 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
     const int block = GF_KNN_BLOCK;
     const int64_t warps_needed = (nquery + kChunk - 1) / kChunk;
     int64_t grid = (warps_needed * 32 + block - 1) / block;
-    grid = std::max<int64_t>(1, std::min<int64_t>(grid, 148LL * (2048 / block)));
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)sm_count() * (2048 / block)));
     if (counters)
         knn_kernel<true><<<(int)grid, block, 0, ctx->stream>>>(nquery, k, t.pos, t.perm, pos_batch, t.phalo,
                                                                pstart, t.owner, t.knn, nearindex, dens,

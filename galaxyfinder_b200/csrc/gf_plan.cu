@@ -110,7 +110,7 @@ __global__ void recentre_kernel(int64_t n, const double *__restrict__ x,
 
 int grid1d(int64_t n) {
     int64_t g = (n + 255) / 256;
-    return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16));
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, sm_count() * 16));
 }
 
 }  // namespace

@@ -185,6 +185,12 @@ __global__ void halo_bg_kernel(int32_t nhalo, const int64_t *__restrict__ pstart
     direct[h] = nt < ndirect ? 1 : 0;
 }
 
+__global__ void bg_eval_kernel(int32_t n, const double *__restrict__ mvir, PotentialParams pp,
+                               double *__restrict__ bg) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) bg[i] = bg_potent_dev(mvir[i], pp);
+}
+
 // bg and direct flags of every halo of t (scratch in ctx->tmp[5]).
 int launch_halo_bg(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const PotentialParams &pp,
                    const int32_t *ntarget_halo, double **bg, int32_t **direct) {
@@ -204,6 +210,14 @@ int launch_halo_bg(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const 
 
 }  // namespace
 
+// The background term of n halo masses as the potential kernels evaluate it.
+int launch_bg_eval(gf_ctx *ctx, int32_t n, const double *mvir, const PotentialParams &pp, double *bg) {
+    if (n <= 0) return GF_OK;
+    bg_eval_kernel<<<(n + 127) / 128, 128, 0, ctx->stream>>>(n, mvir, pp, bg);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
 // Potential at every particle of every halo from the halo's own tree
 // (self potential); outputs in batch order.
 int launch_self_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart,
@@ -216,7 +230,7 @@ int launch_self_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart,
     GF_TRY(launch_halo_bg(ctx, t, pstart, pp, nullptr, &bg, &direct));
     const int block = GF_BH_BLOCK;
     int64_t grid = (t.n + block - 1) / block;
-    grid = std::min<int64_t>(grid, 148LL * (2048 / block));
+    grid = std::min<int64_t>(grid, (int64_t)sm_count() * (2048 / block));
     bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(t.n, t.pos, t.phalo, t.perm, t.pos, t.root,
                                                     t.rend, t.bh, direct, bg, pp, penergy, raw,
                                                     counters);
@@ -234,7 +248,7 @@ int launch_external_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pst
     int32_t *direct;
     GF_TRY(launch_halo_bg(ctx, t, pstart_src, pp, ntarget_halo, &bg, &direct));
     const int block = GF_BH_BLOCK;
-    int64_t grid = std::min<int64_t>((ntarget + block - 1) / block, 148LL * (2048 / block));
+    int64_t grid = std::min<int64_t>((ntarget + block - 1) / block, (int64_t)sm_count() * (2048 / block));
     bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, nullptr, t.pos, t.root,
                                                     t.rend, t.bh, direct, bg, pp, penergy, raw,
                                                     nullptr);

@@ -433,34 +433,55 @@ PathKind path_of(int n) {
 // Table layouts: FFT8: [e^{-2 pi i k/n}, k < n (float2)][G/n (n floats)];
 // RADIX2: [e^{-2 pi i k/n}, k < n/2 (float2)][G/n]; DIRECT: [h_n (n floats)].
 // Twiddles and filters are evaluated in FP64 and rounded once.
-void append_tables(std::vector<float> &tab, int n, double rg_cells, AxisTable &at) {
+
+// Floats of the table of an axis of n cells.
+int64_t axis_table_floats(int n) {
     const PathKind pk = path_of(n);
+    if (pk == PATH_DIRECT) return n;
+    return 2 * (int64_t)(pk == PATH_FFT8 ? n : n / 2) + n;
+}
+
+// Writes the table of one axis into out[0 .. axis_table_floats(n)).  The
+// direct path needs two FP64 work arrays of n entries (g: the spectral
+// factors, c: cos(2 pi j / n)); both plan builders pass their own, so the
+// allocation-free one can keep them on its stack.
+void write_axis_tables(int n, double rg_cells, float *out, double *g, double *c) {
+    const PathKind pk = path_of(n);
+    int64_t k = 0;
+    if (pk != PATH_DIRECT) {
+        const int ntw = pk == PATH_FFT8 ? n : n / 2;
+        for (int i = 0; i < ntw; i++) {
+            const double ang = 2.0 * M_PI * (double)i / (double)n;
+            out[k++] = (float)cos(ang);
+            out[k++] = (float)-sin(ang);
+        }
+        for (int i = 0; i < n; i++) out[k++] = (float)(axis_factor(i, n, rg_cells) / n);
+    } else {
+        // h_m = (1/n) sum_i G_i cos(2 pi (i m mod n) / n): the cosine of each
+        // residue is evaluated once (n calls instead of n^2)
+        for (int i = 0; i < n; i++) {
+            g[i] = axis_factor(i, n, rg_cells);
+            c[i] = cos(2.0 * M_PI * (double)i / (double)n);
+        }
+        for (int mm = 0; mm < n; mm++) {
+            double acc = 0.0;
+            for (int i = 0; i < n; i++) acc += g[i] * c[((long)i * mm) % n];
+            out[k++] = (float)(acc / n);
+        }
+    }
+}
+
+void append_tables(std::vector<float> &tab, int n, double rg_cells, AxisTable &at) {
     // every table starts on a 16-byte boundary: the FFT paths read float2
     // twiddles, and a preceding table may hold an odd number of floats
     while (tab.size() % 4) tab.push_back(0.f);
     at.n = n;
-    at.logn = pk == PATH_DIRECT ? -1 : ilog2_exact(n);
+    at.logn = path_of(n) == PATH_DIRECT ? -1 : ilog2_exact(n);
     at.tab_off = (int64_t)tab.size();
-    if (pk != PATH_DIRECT) {
-        const int ntw = pk == PATH_FFT8 ? n : n / 2;
-        for (int k = 0; k < ntw; k++) {
-            const double ang = 2.0 * M_PI * (double)k / (double)n;
-            tab.push_back((float)cos(ang));
-            tab.push_back((float)-sin(ang));
-        }
-        for (int k = 0; k < n; k++) tab.push_back((float)(axis_factor(k, n, rg_cells) / n));
-    } else {
-        std::vector<double> g(n);
-        for (int k = 0; k < n; k++) g[k] = axis_factor(k, n, rg_cells);
-        for (int mm = 0; mm < n; mm++) {
-            double acc = 0.0;
-            for (int k = 0; k < n; k++) {
-                const long km = ((long)k * mm) % n;
-                acc += g[k] * cos(2.0 * M_PI * (double)km / (double)n);
-            }
-            tab.push_back((float)(acc / n));
-        }
-    }
+    const size_t base = tab.size();
+    tab.resize(base + (size_t)axis_table_floats(n));
+    std::vector<double> work(path_of(n) == PATH_DIRECT ? 2 * (size_t)n : 0);
+    write_axis_tables(n, rg_cells, tab.data() + base, work.data(), work.data() + (work.empty() ? 0 : n));
 }
 
 template <int AXIS, int LOGN>
@@ -484,6 +505,13 @@ int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLau
     if (ntiles > 0x7fffffffLL) {
         set_status(GF_ENOTIMPL, "%lld smoothing tiles exceed one launch", (long long)ntiles);
         return GF_ENOTIMPL;
+    }
+    if (path_of(n) == PATH_FFT8 && pmax != kPencils) {
+        // the FFT kernel decodes every tile as kPencils pencils: a plan cut
+        // for another width would leave pencils unsmoothed
+        set_status(GF_EINVAL, "smoothing plan of %d pencils per tile for a %d-cell FFT axis; the "
+                   "kernel was built for %d", pmax, n, kPencils);
+        return GF_EINVAL;
     }
     switch (path_of(n) == PATH_FFT8 ? ilog2_exact(n) : 0) {
         case 6: return launch_fft<AXIS, 6>(ctx, den, mesh_dev, g, ntiles, axes, tables);
@@ -624,37 +652,6 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
 // point in gf_noalloc.cu.
 namespace gf {
 
-namespace {
-
-// Tables of one axis written straight into `out` (same layouts as
-// append_tables); returns the float count or -1 if `cap` is too small.
-int64_t write_axis_tables(int n, double rg_cells, float *out, int64_t cap) {
-    const PathKind pk = path_of(n);
-    int64_t k = 0;
-    if (pk != PATH_DIRECT) {
-        const int ntw = pk == PATH_FFT8 ? n : n / 2;
-        if (cap < 2 * (int64_t)ntw + n) return -1;
-        for (int i = 0; i < ntw; i++) {
-            const double ang = 2.0 * M_PI * (double)i / (double)n;
-            out[k++] = (float)cos(ang);
-            out[k++] = (float)-sin(ang);
-        }
-        for (int i = 0; i < n; i++) out[k++] = (float)(axis_factor(i, n, rg_cells) / n);
-    } else {
-        if (cap < n || n > kNoAllocMaxAxis) return -1;
-        double g[kNoAllocMaxAxis];
-        for (int i = 0; i < n; i++) g[i] = axis_factor(i, n, rg_cells);
-        for (int mm = 0; mm < n; mm++) {
-            double acc = 0.0;
-            for (int i = 0; i < n; i++) acc += g[i] * cos(2.0 * M_PI * (double)(((long)i * mm) % n) / n);
-            out[k++] = (float)(acc / n);
-        }
-    }
-    return k;
-}
-
-}  // namespace
-
 int smooth_single_build(const gf_mesh_desc &m, unsigned char *blob, size_t cap, SingleMeshPlan *plan) {
     if (m.nx < 1 || m.ny < 1 || m.nz < 1 || !(m.cellsize > 0) || m.nx > kNoAllocMaxAxis ||
         m.ny > kNoAllocMaxAxis || m.nz > kNoAllocMaxAxis) {
@@ -694,14 +691,19 @@ int smooth_single_build(const gf_mesh_desc &m, unsigned char *blob, size_t cap, 
         at[a].logn = path_of(n) == PATH_DIRECT ? -1 : ilog2_exact(n);
         used = (used + 3) & ~int64_t(3);  // 16-byte aligned tables (float2 twiddles)
         at[a].tab_off = used;
-        const int64_t k = write_axis_tables(n, rg_cells, tab + used, tcap - used);
-        if (k < 0) {
+        const int64_t k = axis_table_floats(n);
+        if (k > tcap - used) {
             set_status(GF_EINVAL, "allocation-free smoothing: tables exceed the scratch");
             return GF_EINVAL;
         }
+        double g[kNoAllocMaxAxis], c[kNoAllocMaxAxis];
+        write_axis_tables(n, rg_cells, tab + used, g, c);
         used += k;
-        int pmax = 32;
+        // tiles as smooth_meshes cuts them: kPencils pencils on the FFT path
+        // (the width the FFT kernel decodes), else as many as fit in shared memory
+        int pmax = kPencils;
         if (path_of(n) != PATH_FFT8) {
+            pmax = 32;
             while (pmax > 2 && (size_t)2 * (pmax / 2) * n * sizeof(float2) > 200 * 1024) pmax -= 2;
         }
         const int64_t cx = (m.nx + pmax - 1) / pmax;

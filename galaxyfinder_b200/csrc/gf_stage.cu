@@ -28,7 +28,7 @@ __global__ void vec3_pos_kernel(int64_t n, const double *__restrict__ r, const f
         pos[p] = make_float4((float)r[3 * p], (float)r[3 * p + 1], (float)r[3 * p + 2], m ? m[p] : 0.f);
 }
 
-int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sm_count() * 16)); }
 
 PotentialParams potential_params(float theta2, int ndirect, double potentfact, int add_bg) {
     const gf_physics &ph = physics();
@@ -107,6 +107,15 @@ int gf_knn_density(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_
                       0, &ctx->last_tree));
     GF_TRY(launch_knn(ctx, ctx->last_tree, pstart_dev, reinterpret_cast<const float4 *>(pos4_dev), k,
                       nearindex, dens));
+    return check_device_errors(ctx);
+}
+
+int gf_bg_potent_device(gf_ctx *ctx, int32_t n, const double *mvir_dev, double *bg_dev) {
+    clear_status();
+    if (!ctx || n < 0 || (n > 0 && (!mvir_dev || !bg_dev))) return GF_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    const PotentialParams pp = potential_params(0.5f, 0, physics().potentfact, 1);
+    GF_TRY(launch_bg_eval(ctx, n, mvir_dev, pp, bg_dev));
     return check_device_errors(ctx);
 }
 
@@ -223,7 +232,7 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         }
         const double pf = cfg->potentfact != 0.0 ? cfg->potentfact : physics().potentfact;
         PotentialParams pp = potential_params(cfg->theta2, cfg->ndirect, pf, cfg->add_bg);
-        GF_TRY(launch_self_potential(ctx, ctx->last_tree, b->pstart, pp, o->penergy, nullptr, counters));
+        GF_TRY(launch_self_potential(ctx, ctx->last_tree, b->pstart, pp, o->penergy, o->phi, counters));
     }
     tm.mark();  // 7
     int status = check_device_errors(ctx);

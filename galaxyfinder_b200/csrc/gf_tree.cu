@@ -395,7 +395,7 @@ __global__ void particle_halo(int64_t n, const int64_t *__restrict__ pstart, int
 }
 
 int grid_n(int64_t n) {
-    return (int)std::max<int64_t>(1, std::min<int64_t>((n + kBlock - 1) / kBlock, 148 * 8));
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + kBlock - 1) / kBlock, sm_count() * 8));
 }
 int grid_exact(int64_t n, int block) { return (int)std::max<int64_t>(1, (n + block - 1) / block); }
 

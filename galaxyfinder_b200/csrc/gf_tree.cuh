@@ -30,6 +30,7 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
 int launch_self_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart,
                           const PotentialParams &pp, float *penergy, float *raw,
                           unsigned long long *counters);
+int launch_bg_eval(gf_ctx *ctx, int32_t n, const double *mvir, const PotentialParams &pp, double *bg);
 int launch_external_potential(gf_ctx *ctx, const TreeView &t, const int64_t *pstart_src,
                               int64_t ntarget, const float4 *tpos, const int32_t *thalo,
                               const int32_t *ntarget_halo, const PotentialParams &pp,

@@ -156,7 +156,7 @@ __global__ void scale_kernel(float *__restrict__ den, int64_t n, double factor) 
 
 inline int grid_for(int64_t n, int block) {
     int64_t g = (n + block - 1) / block;
-    const int64_t cap = 148LL * 16;  // 16 resident blocks per SM at most
+    const int64_t cap = (int64_t)sm_count() * 16;  // 16 resident blocks per SM at most
     if (g > cap) g = cap;
     if (g < 1) g = 1;
     return (int)g;

@@ -347,6 +347,11 @@ int gf_knn_density_adjoint(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t 
                            const double *x, const double *y, const double *z, int k, int64_t nq,
                            const int64_t *qidx_dev, const int32_t *nearindex, const double *gdens,
                            double *gx, double *gy, double *gz);
+/* The same term as the stage's potential kernels evaluate it on the device,
+ * for n halo masses (device arrays; stream ordered on ctx).  The device has no
+ * x87 long double, so its intermediates are double where the reference's
+ * (and gf_bg_potent's) are long double. */
+int gf_bg_potent_device(gf_ctx *ctx, int32_t n, const double *mvir_dev, double *bg_dev);
 /* Self potential of every halo: penergy = phi * potentfact + bg(halo mass)
  * (bg only if add_bg); halos with fewer than ndirect particles are summed
  * directly.  raw (optional) receives phi itself. */
@@ -379,6 +384,9 @@ typedef struct gf_stage_out {
     float *dens_mesh;      /* device, n (may be NULL) */
     float *penergy;        /* device, n (may be NULL) */
     double *xr, *yr, *zr;  /* device, n recentred positions (may be NULL) */
+    float *phi;            /* device, n raw tree potential before potentfact and the
+                              background term, i.e. penergy = (float)(phi*potentfact + bg)
+                              (may be NULL) */
 } gf_stage_out;
 
 typedef struct gf_stage_stats {

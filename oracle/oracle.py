@@ -25,7 +25,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 RESTATEMENT = HERE / "_build" / "libgforacle.so"
 REF_DIR = HERE / "_ref"
-REF_SOURCE = Path("/root/reference")
+# the read-only reference tree the recipe compiles; GF_REFERENCE_SOURCE overrides
+# the location this build container mounts it at
+REF_SOURCE = Path(os.environ.get("GF_REFERENCE_SOURCE") or "/root/reference")
 
 _VP, _I, _I64, _F, _D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double
 
@@ -40,9 +42,9 @@ def build(ref: bool = True) -> None:
     reference linked with libgf (make -C oracle linked)."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     if ref and REF_SOURCE.exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REF_SOURCE}", "ref"], check=True)
         if (HERE.parent / "galaxyfinder_b200" / "libgf.a").exists():
-            subprocess.run(["make", "-s", "-C", str(HERE), "linked"], check=True)
+            subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REF_SOURCE}", "linked"], check=True)
 
 
 class Restatement:

@@ -7,6 +7,7 @@ import pytest
 import torch
 
 from galaxyfinder_b200 import _lib, batch, dropin, synth
+from parity import assert_final_rounding
 
 pytestmark = pytest.mark.gpu
 
@@ -67,6 +68,15 @@ def test_c1_mesh_density(c1, restatement):
     rel_lib = np.abs(ref_lib.astype(np.float64) - ref) / ref
     assert rel[lo].max() <= 1.5 * rel_lib[lo].max(), (rel[lo].max(), rel_lib[lo].max())
     assert np.abs(got - ref).max() < 1e-6 * ref.max()
+    # over every particle: the fraction beyond 1e-5 relative (all of them in
+    # the sparse outskirts, where the FP32 mesh's absolute roundoff dominates)
+    # is no larger than a library FP32 FFT's
+    pos = ref > 0
+    frac = np.mean(rel[pos] > 1e-5)
+    frac_lib = np.mean(rel_lib[pos] > 1e-5)
+    print(f"mesh density vs FP64, all {pos.sum()} particles: {frac:.2e} beyond 1e-5 "
+          f"(library FP32 FFT: {frac_lib:.2e}); p99 {np.quantile(rel[pos], 0.99):.2e}")
+    assert frac <= max(1.2 * frac_lib, 1e-4)
 
 
 def _library_fp32_smoothing(d, n3, cell, rg):
@@ -91,10 +101,12 @@ def test_c1_potential(c1, restatement):
     phi = restatement.tree_potential(t["bh"], t["pos"], p.astype(np.float32),
                                      np.zeros(n, np.int32) + t["root"][0],
                                      np.zeros(n, np.int32) + t["rend"][0], None)
+    raw = out.phi.cpu().numpy().astype(np.float64)
+    rel = np.abs(raw - phi) / np.abs(phi)
+    print(f"raw potential vs FP64 walk of the same tree: max rel {rel.max():.2e}, "
+          f"median {np.median(rel):.2e}")
+    assert rel.max() < 1e-6, rel.max()
     ph = dropin.physics()
     m32 = c1["hb"].mass.astype(np.float32)
     bg = dropin.bg_potent(float(np.sum(m32, dtype=np.float64)))
-    expect = phi * ph["potentfact"] + bg
-    got = out.penergy.cpu().numpy().astype(np.float64)
-    err = np.abs(got - expect) / np.abs(phi * ph["potentfact"])
-    assert err.max() < 2e-6, err.max()
+    assert_final_rounding(out.penergy.cpu().numpy(), raw * ph["potentfact"] + bg)

@@ -12,6 +12,7 @@ import pytest
 import torch
 
 from galaxyfinder_b200 import _lib, batch, dropin, synth
+from parity import assert_final_rounding
 from oracle import adjoint as A
 
 pytestmark = pytest.mark.gpu
@@ -34,7 +35,7 @@ def c3(cuda_device):
                xr=np.stack([out.xr.cpu().numpy(), out.yr.cpu().numpy(), out.zr.cpu().numpy()], 1),
                near=out.nearindex[torch.as_tensor(sample, device=out.nearindex.device)].cpu().numpy(),
                dens_sph=out.dens_sph.cpu().numpy()[sample], dens_mesh=out.dens_mesh.cpu().numpy(),
-               penergy=out.penergy.cpu().numpy()[sample])
+               penergy=out.penergy.cpu().numpy()[sample], phi=out.phi.cpu().numpy()[sample])
     nn = st["nnode"]
     res["bh"] = np.zeros(nn, _lib.BH_NODE_DTYPE)
     res["tpos"] = np.zeros((hb.n, 4), np.float32)
@@ -84,6 +85,9 @@ def test_c3_mesh_density(c3, restatement):
     rel = np.abs(got[hi] - ref[hi]) / ref[hi]
     print(f"mesh density vs FP64 (rho > 1e-2 rho_max): max rel {rel.max():.2e}, median {np.median(rel):.2e}")
     assert rel.max() < 1e-5
+    allrel = np.abs(got - ref)[ref > 0] / ref[ref > 0]
+    print(f"mesh density vs FP64, all {len(allrel)} sampled particles: {np.mean(allrel > 1e-5):.2e} "
+          f"beyond 1e-5, p99 {np.quantile(allrel, 0.99):.2e}")
     # the densest cells collect thousands of TSC contributions, summed in
     # float (as the reference's deposit): their rounding grows like sqrt(N) u
     assert np.abs(got - ref).max() < 1e-5 * np.abs(c3["dens_mesh"]).max()
@@ -115,8 +119,11 @@ def test_c3_potential_both_opening_angles(c3, restatement):
     # theta^2 = 0.5: the stage's own potential against an FP64 walk of its tree
     phi = restatement.tree_potential(c3["bh"], c3["tpos"], p32[s], np.zeros(len(s), np.int32) + c3["root"][0],
                                      np.zeros(len(s), np.int32) + c3["rend"][0], None)
-    err = np.abs(c3["penergy"] - (phi * ph["potentfact"] + bg)) / np.abs(phi * ph["potentfact"])
-    assert err.max() < 2e-6, err.max()
+    raw = c3["phi"].astype(np.float64)
+    rel = np.abs(raw - phi) / np.abs(phi)
+    print(f"raw potential vs FP64 walk (theta2=0.5): max rel {rel.max():.2e}, median {np.median(rel):.2e}")
+    assert rel.max() < 1e-6, rel.max()
+    assert_final_rounding(c3["penergy"], raw * ph["potentfact"] + bg)
     e05 = np.abs(phi[:24] - direct) / np.abs(direct)
     # theta = 0.5 (theta^2 = 0.25): the batched potential on its own tree
     ctx = c3["ctx"]
@@ -126,7 +133,9 @@ def test_c3_potential_both_opening_angles(c3, restatement):
     t25 = batch.tree_build_export(ctx, [0, n], pos4, theta2=0.25)
     phi25 = restatement.tree_potential(t25["bh"], t25["pos"], p32[s], np.zeros(len(s), np.int32) + t25["root"][0],
                                        np.zeros(len(s), np.int32) + t25["rend"][0], None)
-    assert np.max(np.abs(raw[s] - phi25) / np.abs(phi25)) < 2e-6
+    rel25 = np.abs(raw[s] - phi25) / np.abs(phi25)
+    print(f"raw potential vs FP64 walk (theta2=0.25): max rel {rel25.max():.2e}")
+    assert rel25.max() < 1e-6
     e025 = np.abs(phi25[:24] - direct) / np.abs(direct)
     print(f"potential vs FP64 direct (24 targets): theta2=0.5 mean {e05.mean():.2e} max {e05.max():.2e}; "
           f"theta2=0.25 mean {e025.mean():.2e} max {e025.max():.2e}")

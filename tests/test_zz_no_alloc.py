@@ -2,7 +2,7 @@
 for callers that cannot allocate device memory: its scratch is a fixed static
 device array instead of context-owned cudaMalloc buffers.  Two calls in a row,
 on different mesh sizes, must reproduce the context-based entry point
-gf_gaussian_smooth on the same meshes.  This file is collected last so a run
+gf_gaussian_smooth on the same meshes, and the oracle's FP64 smoothing.  This file is collected last so a run
 that stops at the first failure has already run every other test."""
 import ctypes
 
@@ -45,7 +45,7 @@ def _with_context(den_host, nx, ny, nz, cell, rg):
     return out
 
 
-def test_noalloc_smoothing_matches_context_entry_point(cuda_device):
+def test_noalloc_smoothing_matches_context_entry_point(cuda_device, restatement):
     stream = torch.cuda.current_stream()
     cases = [((64, 48, 40), 0.004, 0.008), ((37, 64, 128), 0.005, 0.0075)]
     for i, ((nx, ny, nz), cell, rg) in enumerate(cases):
@@ -57,6 +57,11 @@ def test_noalloc_smoothing_matches_context_entry_point(cuda_device):
         got = _logical(d.cpu().numpy(), nx, ny, nz)
         ref = _logical(_with_context(den, nx, ny, nz, cell, rg), nx, ny, nz)
         assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max(), (nx, ny, nz)
+        # and, independently of the context path, the FP64 spectral smoothing
+        # of the oracle on the same mesh
+        _, s64 = restatement.smooth(den, nx, ny, nz, cell, rg)
+        want = _logical(s64, nx, ny, nz)
+        assert np.abs(got - want).max() <= 2e-6 * np.abs(want).max(), (nx, ny, nz)
 
 
 def test_noalloc_rejects_meshes_beyond_its_scratch(cuda_device):
