@@ -49,6 +49,27 @@ CORE_DTYPE = np.dtype([
 ])
 assert CORE_DTYPE.itemsize == 56
 
+# TPtlStruct, NewGalFinder/tree.h:72-77 (56 bytes): a particle of the threaded tree
+TPTL_DTYPE = np.dtype([
+    ("type", "<u4"), ("_pad0", "<u4"), ("sibling", "<u8"), ("x", "<f8"), ("y", "<f8"), ("z", "<f8"),
+    ("mass", "<f8"), ("indx", "<i4"), ("_pad1", "<i4"),
+])
+assert TPTL_DTYPE.itemsize == 56
+
+# TStruct, NewGalFinder/tree.h:79-91 (176 bytes): a node of the threaded tree
+TSTRUCT_DTYPE = np.dtype([
+    ("type", "<u4"), ("_pad0", "<u4"), ("sibling", "<u8"), ("daughter", "<u8"), ("L", "<f8"),
+    ("dist", "<f8"), ("dist2", "<f8"), ("x0", "<f8"), ("y0", "<f8"), ("z0", "<f8"), ("mass", "<f8"),
+    ("Nparticle", "<i4"), ("_pad1", "<i4"), ("monox", "<f8"), ("monoy", "<f8"), ("monoz", "<f8"),
+    ("trQ", "<f8"), ("quad", "<f8", (6,)), ("dist_over_thetasq", "<f8"),
+])
+assert TSTRUCT_DTYPE.itemsize == 176
+
+# particle, NewGalFinder/tree.h:145-149 (40 bytes): a query point
+PARTICLE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("link02", "<f8"),
+                           ("indx", "<i4"), ("_pad", "<i4")])
+assert PARTICLE_DTYPE.itemsize == 40
+
 # gf_mesh_desc (gf.h), 64 bytes
 MESH_DTYPE = np.dtype([
     ("off", "<i8"), ("nx", "<i4"), ("ny", "<i4"), ("nz", "<i4"), ("ptype", "<i4"),
@@ -95,6 +116,7 @@ class StageConfig(ctypes.Structure):
         ("do_mesh", ctypes.c_int32), ("do_potential", ctypes.c_int32), ("ndirect", ctypes.c_int32),
         ("theta2", ctypes.c_float), ("add_bg", ctypes.c_int32), ("q5_asbuilt", ctypes.c_int32),
         ("count_work", ctypes.c_int32), ("potentfact", ctypes.c_double),
+        ("mesh_device_only", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -117,6 +139,8 @@ class StageStats(ctypes.Structure):
         ("knn_nodes", ctypes.c_uint64), ("knn_batches", ctypes.c_uint64),
         ("knn_candidates", ctypes.c_uint64), ("knn_single_inserts", ctypes.c_uint64),
         ("knn_bitonic_merges", ctypes.c_uint64),
+        ("mesh_cells_device", ctypes.c_int64), ("onchip_meshes", ctypes.c_int64),
+        ("onchip_particles", ctypes.c_int64),
     ]
 
 
@@ -159,6 +183,10 @@ SIGNATURES = {
     "gaussian_Smoothing": (None, [_VP, _INT, _INT, _INT, _D, _F]),
     "findsphdensity": (None, [_VP, _INT, _VP, _INT, _VP]),
     "Self_Halo_Potent": (None, [_INT, _VP, _VP, _VP]),
+    "new_Make_Tree_Near": (None, [_VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _INT]),
+    "Make_Tree": (None, [_VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _F, _INT]),
+    "Find_Near": (_INT, [_VP, _INT, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "treeplumpotential": (_F, [_VP, _F, _VP, _VP]),
     "External_Halo_Potent": (None, [_INT, _VP, _VP, _VP, _INT, _VP, _VP]),
     "i_potent_spline": (None, []),
     "lagFindStellarCore": (None, [_VP, _INT, _INT, _VP, _VP, _VP, _INT, _VP, _INT]),

@@ -154,8 +154,24 @@ int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, co
                     const int32_t *hid, const gf_mesh_desc *mesh, const float *den, float *densph,
                     const int32_t *order = nullptr);
 int launch_scale(gf_ctx *ctx, float *den, int64_t ncells, double factor);
+// Halos whose whole mesh stage (TSC deposit, smoothing, findDen) runs on
+// chip: meshes of kOnChipMesh^3 cells held in the distributed shared memory
+// of one thread-block cluster, never written to device memory.  Their mesh
+// descriptors carry ptype == kMeshOnChip, which the device-memory kernels skip.
+constexpr int kOnChipMesh = 64;
+constexpr int32_t kMeshOnChip = -1;
+struct OnChipMeshes {
+    int32_t nmesh = 0;
+    const int32_t *halos_host = nullptr;  // [nmesh] halo ids (host; uploaded with the tables)
+    int32_t ptype = GF_TYPE_ALL;          // particles deposited
+    const int64_t *pstart = nullptr;      // device, batch halo starts
+    const double *x = nullptr, *y = nullptr, *z = nullptr, *mass = nullptr;  // device, batch order
+    const int32_t *type = nullptr;
+    float volfold = 1.f;                  // 1 or the exact power-of-two volfact
+    float *densph = nullptr;              // device, mesh density at every particle of these halos
+};
 int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
-                  const gf_mesh_desc *mesh_dev, float *den);
+                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip = nullptr);
 
 // Single-mesh smoothing plan in one contiguous byte blob (see gf_smooth.cu):
 // [mesh desc | 3 axis tables | per axis: halo list, tile prefix | tables].

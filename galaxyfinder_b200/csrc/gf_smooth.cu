@@ -23,7 +23,9 @@
 #include <map>
 #include <utility>
 
-#include "gf_internal.cuh"
+#include <cooperative_groups.h>
+
+#include "gf_tsc_weights.cuh"
 
 namespace gf {
 
@@ -326,6 +328,207 @@ __device__ __forceinline__ void fft_filter_ifft(float2 *b0, float2 *b1, int npai
     }
 }
 
+// ---------------------------------------------------------------- on-chip meshes
+// The whole mesh stage of a 64^3 mesh inside one cluster of 8 CTAs: CTA r
+// holds z planes [8r, 8r + 8) in shared memory (rows padded to 65 floats, so
+// columns along y and x-consecutive lanes are conflict-free), and reaches the
+// other planes through distributed shared memory.  Per mesh: zero the slabs,
+// deposit the TSC weights (the reference's arithmetic, float atomics into the
+// owning CTA's slab), filter along x and y (local planes) and along z (columns
+// read from all eight CTAs), then interpolate at every particle.  Each filter
+// pass moves tiles of 128 real pencils into a padded buffer and runs the same
+// Stockham FFT -> filter -> inverse FFT as the device-memory kernels.  Nothing
+// of the mesh touches device memory; a cluster loops over meshes.
+namespace oc {
+constexpr int kN = kOnChipMesh;                 // 64 cells per axis
+constexpr int kCtas = 8;                        // CTAs per cluster
+constexpr int kPlanes = kN / kCtas;             // z planes per CTA
+constexpr int kRow = kN + 1;                    // padded row stride (floats)
+constexpr int kPlane = kN * kRow;               // plane stride (floats)
+constexpr int kSlab = kPlanes * kPlane;         // floats per CTA
+constexpr int kOcThreads = 512;
+constexpr int kTilePencils = 128;               // real pencils per FFT tile
+constexpr int kPairs = kTilePencils / 2;
+constexpr int kTiles = kPlanes * kN / kTilePencils;  // tiles per pass per CTA (4)
+using L = FftLayout<kN>;
+constexpr size_t kSmem = (size_t)kSlab * sizeof(float) + 2 * (size_t)kPairs * L::SN * sizeof(float2);
+static_assert(kOcThreads == kPairs * (kN / 8), "one radix-8 butterfly per thread and pass");
+static_assert(kSmem <= 227 * 1024, "shared memory per CTA");
+}  // namespace oc
+
+struct OnChipArgs {
+    int32_t nmesh;
+    const int32_t *halos;
+    int32_t ptype;
+    const int64_t *pstart;
+    const double *x, *y, *z, *mass;
+    const int32_t *type;
+    const gf_mesh_desc *mesh;
+    const AxisTable *axes;
+    const float *tables;
+    float volfold;
+    float *densph;
+    int *err;
+};
+
+// One filter pass over the tile of real pencils whose element (p, s) lives
+// at address(p, s) in (local or remote) shared memory.
+template <class Addr>
+__device__ __forceinline__ void onchip_tile(float2 *b0, float2 *b1, const AxisTable &at,
+                                            const float *__restrict__ tables, Addr address) {
+    using namespace oc;
+    float *fa = reinterpret_cast<float *>(b0);
+    constexpr int PER = kTilePencils * kN / kOcThreads;  // 16
+    float v[PER];
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+        const int e = threadIdx.x + r * kOcThreads;
+        v[r] = *address(e & (kTilePencils - 1), e >> 7);
+    }
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+        const int e = threadIdx.x + r * kOcThreads;
+        const int p = e & (kTilePencils - 1), s = e >> 7;
+        fa[2 * L::at(p >> 1, s) + (p & 1)] = v[r];
+    }
+    __syncthreads();
+    const float2 *tw = reinterpret_cast<const float2 *>(tables + at.tab_off);
+    const float *filt = tables + at.tab_off + 2 * kN;
+    fft_filter_ifft<6>(b0, b1, kPairs, tw, filt);
+    const float *fs = reinterpret_cast<const float *>(b0);
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+        const int e = threadIdx.x + r * kOcThreads;
+        const int p = e & (kTilePencils - 1), s = e >> 7;
+        *address(p, s) = fs[2 * L::at(p >> 1, s) + (p & 1)];
+    }
+    __syncthreads();
+}
+
+__global__ void __cluster_dims__(oc::kCtas, 1, 1) __launch_bounds__(oc::kOcThreads, 1)
+mesh_onchip_kernel(OnChipArgs a) {
+    using namespace oc;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    extern __shared__ float4 smem_f4[];
+    float *slab = reinterpret_cast<float *>(smem_f4);
+    float2 *b0 = reinterpret_cast<float2 *>(slab + kSlab);
+    float2 *b1 = b0 + kPairs * L::SN;
+    // the slab of CTA r of the cluster (distributed shared memory window)
+    auto slabs = [&](int r) { return cluster.map_shared_rank(slab, r); };
+    const int nclusters = gridDim.x / kCtas;
+    for (int mi = blockIdx.x / kCtas; mi < a.nmesh; mi += nclusters) {
+        const int h = a.halos[mi];
+        const gf_mesh_desc m = a.mesh[h];
+        for (int e = threadIdx.x; e < kSlab; e += kOcThreads) slab[e] = 0.f;
+        cluster.sync();
+        // ---- TSC deposit (tsc_omp2.c:166-506), into the CTA owning each plane
+        const int64_t p0 = a.pstart[h], p1 = a.pstart[h + 1];
+        for (int64_t p = p0 + rank * kOcThreads + threadIdx.x; p < p1; p += kCtas * kOcThreads) {
+            if (a.ptype != GF_TYPE_ALL && (a.type ? a.type[p] : GF_TYPE_DM) != a.ptype) continue;
+            TscStencil st;
+            float xd1, yd1, zd1;
+            tsc_cells(a.x[p], a.y[p], a.z[p], m, st, xd1, yd1, zd1);
+            if (!tsc_in_mesh(st, m)) {
+                atomicOr(a.err, GF_ERRBIT_RANGE);
+                continue;
+            }
+            tsc_deposit_weights(st, xd1, yd1, zd1, a.mass[p]);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const int k = (int)st.k[c];
+                float *dst = slabs(k / kPlanes) + (k % kPlanes) * kPlane;
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+                        atomicAdd(dst + (int)st.j[b] * kRow + (int)st.i[i], tsc_deposit_value(st, i, b, c, a.volfold));
+                }
+            }
+        }
+        cluster.sync();
+        // ---- filter along x: the CTA's 512 rows (plane, y), 128 per tile
+        const AxisTable ax = a.axes[3 * h], ay = a.axes[3 * h + 1], az = a.axes[3 * h + 2];
+        for (int t = 0; t < kTiles; t++) {
+            onchip_tile(b0, b1, ax, a.tables, [&](int p, int s) {
+                const int row = t * kTilePencils + p;
+                return slab + (row / kN) * kPlane + (row % kN) * kRow + s;
+            });
+        }
+        // ---- along y: columns (plane, x) of the CTA's planes
+        for (int t = 0; t < kTiles; t++) {
+            onchip_tile(b0, b1, ay, a.tables, [&](int p, int s) {
+                const int col = t * kTilePencils + p;
+                return slab + (col / kN) * kPlane + s * kRow + (col % kN);
+            });
+        }
+        cluster.sync();
+        // ---- along z: the CTA's share of the 64 x 64 columns, through all slabs
+        for (int t = 0; t < kTiles; t++) {
+            onchip_tile(b0, b1, az, a.tables, [&](int p, int s) {
+                const int col = rank * (kN * kN / kCtas) + t * kTilePencils + p;
+                return slabs(s / kPlanes) + (s % kPlanes) * kPlane + (col / kN) * kRow + (col % kN);
+            });
+        }
+        cluster.sync();
+        // ---- findDen (tsc_omp2.c:40-163) at every particle of the halo
+        for (int64_t p = p0 + rank * kOcThreads + threadIdx.x; p < p1; p += kCtas * kOcThreads) {
+            TscStencil st;
+            float xd1, yd1, zd1;
+            tsc_cells(a.x[p], a.y[p], a.z[p], m, st, xd1, yd1, zd1);
+            if (!tsc_in_mesh(st, m)) {
+                atomicOr(a.err, GF_ERRBIT_RANGE);
+                a.densph[p] = 0.f;
+                continue;
+            }
+            tsc_interp_weights(st, xd1, yd1, zd1);
+            float density = 0.f;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const int k = (int)st.k[c];
+                const float *src = slabs(k / kPlanes) + (k % kPlanes) * kPlane;
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+                        density = tsc_interp_add(density, src[(int)st.j[b] * kRow + (int)st.i[i]], st, i, b, c);
+                }
+            }
+            a.densph[p] = density;
+        }
+        cluster.sync();  // before the next mesh clears the slabs
+    }
+}
+
+int launch_onchip(gf_ctx *ctx, const OnChipArgs &a) {
+    if (a.nmesh <= 0) return GF_OK;
+    GF_CUDA_TRY(cudaFuncSetAttribute(mesh_onchip_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)oc::kSmem));
+    // as many clusters as can be resident at once (each loops over meshes)
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = oc::kCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(oc::kOcThreads);
+    cfg.gridDim = dim3(oc::kCtas * 64);
+    cfg.dynamicSmemBytes = oc::kSmem;
+    cfg.stream = ctx->stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, mesh_onchip_kernel, &cfg) != cudaSuccess || nclusters < 1) {
+        cudaGetLastError();
+        nclusters = std::max(1, sm_count() / oc::kCtas);
+    }
+    nclusters = std::min(nclusters, a.nmesh);
+    mesh_onchip_kernel<<<nclusters * oc::kCtas, oc::kOcThreads, oc::kSmem, ctx->stream>>>(a);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
 constexpr int kPencils = GF_FFT_PENCILS;  // real pencils per FFT tile (2 per complex pencil)
 
 template <int AXIS, int LOGN>
@@ -532,8 +735,9 @@ int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLau
 }  // namespace
 
 int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
-                  const gf_mesh_desc *mesh_dev, float *den) {
+                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip) {
     if (nhalo <= 0) return GF_OK;
+    const int32_t non_chip = onchip ? onchip->nmesh : 0;  // meshes on chip
     std::vector<AxisTable> axes(3 * (size_t)nhalo);
     std::vector<float> tables;
     std::map<std::pair<int, double>, AxisTable> cache;
@@ -568,6 +772,7 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
     for (int a = 0; a < 3; a++) {
         for (int h = 0; h < nhalo; h++) {
             const gf_mesh_desc &m = mesh_host[h];
+            if (m.ptype == kMeshOnChip) continue;  // smoothed on chip
             const int dims[3] = {m.nx, m.ny, m.nz};
             const int n = dims[a];
             const int key_n = path_of(n) == PATH_FFT8 ? n : -1;
@@ -602,11 +807,13 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
             g.start.push_back(g.start.back() + c);
         }
     }
-    // one staging buffer: [axes | tables | per group: halos, starts]
+    // one staging buffer: [axes | tables | on-chip halos | per group: halos, starts]
     auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
     size_t off = align(axes.size() * sizeof(AxisTable));
     const size_t off_tab = off;
     off = align(off + tables.size() * sizeof(float));
+    const size_t off_chip = off;
+    off = align(off + (size_t)non_chip * sizeof(int32_t));
     std::vector<size_t> off_h(groups.size()), off_s(groups.size());
     for (size_t i = 0; i < groups.size(); i++) {
         off_h[i] = off;
@@ -622,6 +829,7 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
     GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     memcpy(hbuf, axes.data(), axes.size() * sizeof(AxisTable));
     memcpy(hbuf + off_tab, tables.data(), tables.size() * sizeof(float));
+    if (non_chip) memcpy(hbuf + off_chip, onchip->halos_host, (size_t)non_chip * sizeof(int32_t));
     for (size_t i = 0; i < groups.size(); i++) {
         memcpy(hbuf + off_h[i], groups[i].halos.data(), groups[i].halos.size() * sizeof(int32_t));
         memcpy(hbuf + off_s[i], groups[i].start.data(), groups[i].start.size() * sizeof(int64_t));
@@ -640,6 +848,25 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
         if (g.axis == 0) GF_TRY(launch_group<0>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
         else if (g.axis == 1) GF_TRY(launch_group<1>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
         else GF_TRY(launch_group<2>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
+    }
+    if (non_chip) {
+        OnChipArgs a;
+        a.nmesh = non_chip;
+        a.halos = reinterpret_cast<const int32_t *>(dbuf + off_chip);
+        a.ptype = onchip->ptype;
+        a.pstart = onchip->pstart;
+        a.x = onchip->x;
+        a.y = onchip->y;
+        a.z = onchip->z;
+        a.mass = onchip->mass;
+        a.type = onchip->type;
+        a.mesh = mesh_dev;
+        a.axes = d_axes;
+        a.tables = d_tab;
+        a.volfold = onchip->volfold;
+        a.densph = onchip->densph;
+        a.err = ctx->d_err;
+        GF_TRY(launch_onchip(ctx, a));
     }
     return GF_OK;
 }

@@ -160,10 +160,25 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
     float4 *pos = reinterpret_cast<float4 *>(t2 + 3 * dbytes);  // 256-byte aligned
     // mesh plan from the recentred extents
     std::vector<gf_mesh_desc> mesh((size_t)std::max(nh, 1));
-    int64_t cells = 0;
+    int64_t cells = 0, dev_cells = 0;
+    std::vector<int32_t> onchip_halos;
     if (cfg->do_mesh) {
         int sp = gf_plan_meshes(nh, extent.data(), &cfg->mesh, mesh.data(), &cells);
         if (sp != GF_OK) return sp;
+        // 64^3 meshes run their whole mesh stage on chip; the others are laid
+        // out in device memory
+        for (int32_t h = 0; h < nh; h++) {
+            gf_mesh_desc &m = mesh[h];
+            if (!cfg->mesh_device_only && m.nx == kOnChipMesh && m.ny == kOnChipMesh && m.nz == kOnChipMesh) {
+                m.ptype = kMeshOnChip;
+                m.off = 0;
+                onchip_halos.push_back(h);
+                continue;
+            }
+            m.off = dev_cells;
+            dev_cells += mesh_cells(m);
+            dev_cells = (dev_cells + 63) & ~int64_t(63);  // 256-byte aligned mesh starts
+        }
     }
     const size_t frame_bytes = frame.size() * sizeof(double);
     const size_t mesh_bytes = mesh.size() * sizeof(gf_mesh_desc);
@@ -201,17 +216,35 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
     tm.mark();  // 3
     // ---- 4. TSC mesh -> smoothing -> findDen
     if (cfg->do_mesh) {
-        GF_TRY(ctx->tmp[3].reserve(sizeof(float) * (size_t)std::max<int64_t>(cells, 1)));
+        GF_TRY(ctx->tmp[3].reserve(sizeof(float) * (size_t)std::max<int64_t>(dev_cells, 1)));
         float *den = ctx->tmp[3].as<float>();
-        GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * cells, s));
+        GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * dev_cells, s));
         const double vf = tsc_volfact();
         // batch order: the deposit's float sums in octree order were faster
         // (2.73 -> 2.34 ms) but put the densest cells of the 5e7-particle
         // cluster 1.04e-5 from an FP64 deposit, past the 1e-5 target
         GF_TRY(launch_tsc_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, mesh_dev, den, vf));
-        if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, cells, vf));
+        if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, dev_cells, vf));
         tm.mark();  // 4
-        GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den));
+        OnChipMeshes oc;
+        if (!onchip_halos.empty()) {
+            if (!o->dens_mesh || !volfact_folds(vf)) {
+                set_status(GF_EINVAL, "on-chip meshes need dens_mesh and a power-of-two volfact");
+                return GF_EINVAL;
+            }
+            oc.nmesh = (int32_t)onchip_halos.size();
+            oc.halos_host = onchip_halos.data();
+            oc.ptype = cfg->mesh.ptype;
+            oc.pstart = b->pstart;
+            oc.x = xr;
+            oc.y = yr;
+            oc.z = zr;
+            oc.mass = b->mass;
+            oc.type = b->type;
+            oc.volfold = (float)vf;
+            oc.densph = o->dens_mesh;
+        }
+        GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den, &oc));
         tm.mark();  // 5
         if (o->dens_mesh)
             GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh,
@@ -242,6 +275,14 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         st->nhalo = nh;
         st->nnode = need_tree ? ctx->last_tree.nnode : 0;
         st->mesh_cells = cells;
+        st->mesh_cells_device = dev_cells;
+        st->onchip_meshes = (int64_t)onchip_halos.size();
+        std::vector<int64_t> ps_host;
+        if (!onchip_halos.empty()) {
+            ps_host.resize((size_t)nh + 1);
+            cudaMemcpy(ps_host.data(), b->pstart, ps_host.size() * sizeof(int64_t), cudaMemcpyDeviceToHost);
+            for (int32_t h : onchip_halos) st->onchip_particles += ps_host[h + 1] - ps_host[h];
+        }
         st->ms_recentre = tm.ms(0);
         st->ms_tree = tm.ms(1);
         st->ms_knn = tm.ms(2);

@@ -7,37 +7,11 @@
 // the same FP64 positions.  The only difference left in the deposited mesh
 // is the order in which float atomics sum the contributions of different
 // particles to one cell.
-#include "gf_internal.cuh"
+#include "gf_tsc_weights.cuh"
 
 namespace gf {
 
 namespace {
-
-struct Stencil {
-    int64_t i[3], j[3], k[3];
-    float wx[3], wy[3], wz[3];
-};
-
-// Position -> mesh coordinate, nearest node and float offset, as
-// tsc_omp2.c:303-314 (XYZDBL build: double xp, rint, float remainder).
-__device__ __forceinline__ void tsc_axis(double pos, double origin, double cellsize,
-                                         int64_t &near1, int64_t &near2, int64_t &near3,
-                                         float &d1) {
-    double xp = (pos - origin) / cellsize;
-    double nr = rint(xp);
-    float rem = (float)(xp - nr);
-    int64_t sgn = (int64_t)copysignf(1.f, rem);
-    near1 = (int64_t)nr;
-    near2 = near1 + sgn;
-    near3 = near1 - sgn;
-    d1 = fabsf(rem);
-}
-
-__device__ __forceinline__ bool in_mesh(const Stencil &s, const gf_mesh_desc &m) {
-    // the stencil spans [near-1, near+1] on every axis
-    return s.i[0] >= 1 && s.i[0] + 1 < m.nx && s.j[0] >= 1 && s.j[0] + 1 < m.ny &&
-           s.k[0] >= 1 && s.k[0] + 1 < m.nz;
-}
 
 __global__ void tsc_deposit_kernel(int64_t n, const double *__restrict__ x,
                                    const double *__restrict__ y, const double *__restrict__ z,
@@ -54,31 +28,14 @@ __global__ void tsc_deposit_kernel(int64_t n, const double *__restrict__ x,
         const int64_t p = order ? (int64_t)order[t] : t;
         const gf_mesh_desc m = mesh[hid ? hid[p] : 0];
         if (m.ptype != GF_TYPE_ALL && (type ? type[p] : GF_TYPE_DM) != m.ptype) continue;
-        Stencil s;
+        TscStencil s;
         float xd1, yd1, zd1;
-        tsc_axis(x[p], m.xmin, m.cellsize, s.i[0], s.i[1], s.i[2], xd1);
-        tsc_axis(y[p], m.ymin, m.cellsize, s.j[0], s.j[1], s.j[2], yd1);
-        tsc_axis(z[p], m.zmin, m.cellsize, s.k[0], s.k[1], s.k[2], zd1);
-        if (!in_mesh(s, m)) {
+        tsc_cells(x[p], y[p], z[p], m, s, xd1, yd1, zd1);
+        if (!tsc_in_mesh(s, m)) {
             atomicOr(err, GF_ERRBIT_RANGE);
             continue;
         }
-        // tsc_omp2.c:335-343: mass folded into the x weights, double
-        // intermediates rounded to float at each assignment.
-        const double pmas0 = mass[p];
-        const double p05 = pmas0 * 0.5;
-        float wx1 = (float)((0.75 - (double)(xd1 * xd1)) * pmas0);
-        float wy1 = (float)(0.75 - (double)(yd1 * yd1));
-        float wz1 = (float)(0.75 - (double)(zd1 * zd1));
-        float wx3 = (float)(p05 * (0.25 + (double)xd1 * ((double)xd1 - 1.)));
-        float wx2 = (float)((double)wx3 + pmas0 * (double)xd1);
-        float wy3 = (float)(0.5 * (0.25 + (double)yd1 * ((double)yd1 - 1.)));
-        float wy2 = wy3 + yd1;
-        float wz3 = (float)(0.5 * (0.25 + (double)zd1 * ((double)zd1 - 1.)));
-        float wz2 = wz3 + zd1;
-        s.wx[0] = wx1; s.wx[1] = wx2; s.wx[2] = wx3;
-        s.wy[0] = wy1; s.wy[1] = wy2; s.wy[2] = wy3;
-        s.wz[0] = wz1; s.wz[1] = wz2; s.wz[2] = wz3;
+        tsc_deposit_weights(s, xd1, yd1, zd1, mass[p]);
         const int64_t mx = 2 * (m.nx / 2 + 1);
         float *mesh_h = den + m.off;
 #pragma unroll
@@ -87,10 +44,9 @@ __global__ void tsc_deposit_kernel(int64_t n, const double *__restrict__ x,
             for (int b = 0; b < 3; b++) {
 #pragma unroll
                 for (int a = 0; a < 3; a++) {
-                    float wxy = s.wx[a] * s.wy[b];
-                    float w = wxy * s.wz[c];
                     // volfold is 1 or an exact power of two (see launch_tsc_deposit)
-                    atomicAdd(mesh_h + s.i[a] + mx * (s.j[b] + (int64_t)m.ny * s.k[c]), w * volfold);
+                    atomicAdd(mesh_h + s.i[a] + mx * (s.j[b] + (int64_t)m.ny * s.k[c]),
+                              tsc_deposit_value(s, a, b, c, volfold));
                 }
             }
         }
@@ -107,26 +63,16 @@ __global__ void find_den_kernel(int64_t n, const double *__restrict__ x,
          t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t p = order ? (int64_t)order[t] : t;  // octree order: shared stencil lines
         const gf_mesh_desc m = mesh[hid ? hid[p] : 0];
-        Stencil s;
+        if (m.ptype == kMeshOnChip) continue;  // interpolated on chip
+        TscStencil s;
         float xd1, yd1, zd1;
-        tsc_axis(x[p], m.xmin, m.cellsize, s.i[0], s.i[1], s.i[2], xd1);
-        tsc_axis(y[p], m.ymin, m.cellsize, s.j[0], s.j[1], s.j[2], yd1);
-        tsc_axis(z[p], m.zmin, m.cellsize, s.k[0], s.k[1], s.k[2], zd1);
-        if (!in_mesh(s, m)) {
+        tsc_cells(x[p], y[p], z[p], m, s, xd1, yd1, zd1);
+        if (!tsc_in_mesh(s, m)) {
             atomicOr(err, GF_ERRBIT_RANGE);
             densph[p] = 0.f;
             continue;
         }
-        // tsc_omp2.c:75-83
-        s.wx[0] = (float)(0.75 - (double)(xd1 * xd1));
-        s.wy[0] = (float)(0.75 - (double)(yd1 * yd1));
-        s.wz[0] = (float)(0.75 - (double)(zd1 * zd1));
-        s.wx[2] = (float)(0.5 * (0.25 + (double)xd1 * ((double)xd1 - 1.)));
-        s.wx[1] = s.wx[2] + xd1;
-        s.wy[2] = (float)(0.5 * (0.25 + (double)yd1 * ((double)yd1 - 1.)));
-        s.wy[1] = s.wy[2] + yd1;
-        s.wz[2] = (float)(0.5 * (0.25 + (double)zd1 * ((double)zd1 - 1.)));
-        s.wz[1] = s.wz[2] + zd1;
+        tsc_interp_weights(s, xd1, yd1, zd1);
         const int64_t mx = 2 * (m.nx / 2 + 1);
         const float *mesh_h = den + m.off;
         // tsc_omp2.c:96-124: for each z plane, y rows in order 1,2,3, x in
@@ -138,9 +84,8 @@ __global__ void find_den_kernel(int64_t n, const double *__restrict__ x,
             for (int b = 0; b < 3; b++) {
 #pragma unroll
                 for (int a = 0; a < 3; a++) {
-                    float wxy = s.wx[a] * s.wy[b];
-                    float v = __ldg(mesh_h + s.i[a] + mx * (s.j[b] + (int64_t)m.ny * s.k[c]));
-                    density += (v * wxy) * s.wz[c];
+                    const float v = __ldg(mesh_h + s.i[a] + mx * (s.j[b] + (int64_t)m.ny * s.k[c]));
+                    density = tsc_interp_add(density, v, s, a, b, c);
                 }
             }
         }

@@ -101,6 +101,34 @@ void findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, i
 void lagFindStellarCore(SimpleBasicParticleType *bp, int np, int Numnear, float *densph,
                         Coretype **Core, int *NumCore, int maxnumcore, long long *nearindex,
                         int ptype);
+/* NewGalFinder/nnost.c:199 (new_Make_Tree_Near) and ost.c:642 (Make_Tree).
+ * Build libgf's centre-of-mass octree of ptl[0..np) on the GPU and write it
+ * into TREE_START[0..nnode) in the reference's threaded layout (tree.h:72-91),
+ * relinking ptl[].sibling: a node's daughter is its first offspring (its
+ * loose particles first, then its child nodes), each offspring's sibling the
+ * next, the last one's sibling the node's sibling.  mass, monox/y/z, dist
+ * (= max |x - com|), dist2, quad, trQ and Nparticle are FP64 moments of the
+ * node's particles; Make_Tree also sets dist_over_thetasq = dist2/thetasq.
+ * The node count must fit nnode (GF_ENOMEM otherwise).  recursiveflag is
+ * accepted and ignored: the build is the same for every mode. */
+void new_Make_Tree_Near(TStruct *TREE_START, size_t nnode, TPtlStruct *ptl, size_t np,
+                        int recursiveflag);
+void Make_Tree(TStruct *TREE_START, size_t nnode, TPtlStruct *ptl, size_t np, float thetasq,
+               int recursiveflag);
+/* NewGalFinder/nnost.c:375.  The Num_neighbor (<= 32) nearest particles of
+ * *point among the tree's particles, self included: indices into ptl,
+ * squared distances (FP64, (dx*dx + dy*dy) + dz*dz) and masses in ascending
+ * distance (equal distances by index), *maxr = sqrtf(k-th squared distance);
+ * returns their number.  Thread safe.  The first call on a tree answers every
+ * particle of the tree in one launch; calls at a particle's exact position
+ * then copy its row, other points run a one-point launch.  A tree the caller
+ * built by other code is read by walking its threads. */
+int Find_Near(particle *point, int Num_neighbor, TStruct *tree, TPtlStruct *ptl, float *maxr,
+              long long *nearindx, double *DIST2, float *MASS);
+/* NewGalFinder/ost.c:226.  Raw Barnes-Hut potential of the tree's particles
+ * at *p (opening |p - com|^2 < dist2/theta2, particle terms with r > 0, no
+ * potentfact), on the GPU with the same batching as Find_Near.  Thread safe. */
+float treeplumpotential(particle *p, float theta2, TStruct *tree, TPtlStruct *ptl);
 /* NewGalFinder/subhaloden.mod6.c:416.  Density peaks on the kNN graph:
  * particles with den > PEAKTHRESHOLD (stars only when jflag is 1) whose kNN
  * list (neighbor, np*numneigh) holds no denser particle, written to *Core in
@@ -376,6 +404,10 @@ typedef struct gf_stage_config {
     int32_t q5_asbuilt;    /* reproduce ost.c:571's y*x in place of y*z */
     int32_t count_work;    /* with stats: also count kNN/potential work (slower) */
     double potentfact;     /* 0: from gf_get_physics() */
+    int32_t mesh_device_only; /* 1: every mesh through device memory; 0: 64^3 meshes run
+                                 their whole mesh stage in one thread-block cluster's
+                                 shared memory */
+    int32_t reserved;
 } gf_stage_config;
 
 typedef struct gf_stage_out {
@@ -397,6 +429,9 @@ typedef struct gf_stage_stats {
     /* kNN work: nodes tested, 32-wide leaf batches, candidates passing the
      * float filter, candidates inserted one by one, bitonic batch merges */
     uint64_t knn_nodes, knn_batches, knn_candidates, knn_single_inserts, knn_bitonic_merges;
+    /* meshes: floats laid out in device memory (mesh_cells counts every
+     * planned mesh), and the meshes and particles of the on-chip path */
+    int64_t mesh_cells_device, onchip_meshes, onchip_particles;
 } gf_stage_stats;
 
 /* stats may be NULL; when given, per-phase CUDA-event times are filled in. */

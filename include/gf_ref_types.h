@@ -8,7 +8,16 @@
  *   Coretype                 NewGalFinder/tree.h:204-213   56 bytes
  *   Kptype                   NewGalFinder/subhaloden.mod6.c:73-77   48 bytes
  *   Coresorttype             NewGalFinder/subhaloden.mod6.c:298-301 16 bytes
+ *   TPtlStruct               NewGalFinder/tree.h:72-77     56 bytes
+ *   TStruct                  NewGalFinder/tree.h:79-91     176 bytes
+ *   particle                 NewGalFinder/tree.h:145-149   40 bytes
  *
+ * TPtlStruct and TStruct are the threaded tree of the reference's kNN and
+ * potential walks (nnost.c and ost.c both include tree.h, and both read the
+ * node size from `dist`): a node's `daughter` points to its first offspring
+ * (a node or a particle), every offspring's `sibling` to the next one, and the
+ * last offspring's `sibling` to the node's own sibling; `type` tells nodes
+ * (GF_TYPE_TREE) from particles (GF_TYPE_PTL).
  * Only the layout is shared; no reference code is included. */
 #ifndef GF_REF_TYPES_H
 #define GF_REF_TYPES_H
@@ -57,6 +66,35 @@ typedef struct Coresorttype {
     int nmem;
     Coretype *core;
 } Coresorttype;
+
+typedef struct TPtlStruct {
+    unsigned int type;
+    void *sibling;
+    double x, y, z;
+    double mass;
+    int indx;
+} TPtlStruct;
+
+typedef struct TStruct {
+    unsigned int type;
+    void *sibling;
+    void *daughter;
+    double L;
+    double dist, dist2;        /* node size max|x - com| and its square */
+    double x0, y0, z0;
+    double mass;
+    int Nparticle;
+    double monox, monoy, monoz; /* centre of mass */
+    double trQ;
+    double quad[6];            /* xx, yy, zz, xy, xz, yz second moments about the COM */
+    double dist_over_thetasq;
+} TStruct;
+
+typedef struct particle {
+    double x, y, z;
+    double link02;
+    int indx;
+} particle;
 
 /* Bound flags of CheckSelfTE/CheckExternalTE (subhaloden.mod6.c:32-33) */
 #define GF_BOUND 1

@@ -138,3 +138,26 @@ def test_stage_stats(run):
     assert st["nparticle"] == run["hb"].n and st["nhalo"] == run["hb"].nhalo
     assert st["pp_interactions"] > 0 and st["pc_interactions"] > 0
     assert st["mesh_cells"] > 0 and st["nnode"] > 0
+
+
+def test_onchip_meshes_match_device_meshes(run):
+    """The 64^3 meshes kept in a cluster's shared memory give the mesh density
+    of the device-memory path (same arithmetic; float atomics sum the deposit
+    in another order)."""
+    hb = run["hb"]
+    ctx = batch.Context(0)
+    db = batch.DeviceBatch.from_halobatch(hb)
+    on = batch.stage_run(ctx, db, batch.stage_config(knn_k=0, do_potential=False))
+    off = batch.stage_run(ctx, db, batch.stage_config(knn_k=0, do_potential=False, mesh_device_only=True))
+    torch.cuda.synchronize()
+    a, b = on.dens_mesh.cpu().numpy(), off.dens_mesh.cpu().numpy()
+    ps = hb.pstart
+    for h in range(hb.nhalo):
+        sa, sb = a[ps[h]:ps[h + 1]], b[ps[h]:ps[h + 1]]
+        assert np.abs(sa - sb).max() <= 2e-6 * np.abs(sb).max(), h
+    r = np.stack([on.xr.cpu().numpy(), on.yr.cpu().numpy(), on.zr.cpu().numpy()], 1)
+    ext = np.array([r[ps[h]:ps[h + 1]].max(0) for h in range(hb.nhalo)])
+    mesh, _ = batch.plan_meshes(ext, run["cfg"].mesh)
+    n64 = int(np.sum(mesh["nx"] == 64))
+    assert n64 >= 5  # the catalogue exercises the on-chip path
+    ctx.close()
