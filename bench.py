@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunks", type=int, default=8,
                     help="halo chunks (streams) of the pipelined stage")
+    ap.add_argument("--configs", action="store_true",
+                    help="also time the single-halo workloads (131072-particle halo, 5e7 cluster, 1e7 mixture)")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the comparison of sampled halos with the oracle")
     return ap.parse_args()
@@ -299,6 +301,52 @@ def catalogue_mesh_cells(hb) -> int:
     from oracle import plan as oplan
     ext = np.array([recentred_halo(hb, h)[0].max(0) for h in range(hb.nhalo)])
     return int(oplan.plan(ext, **MESH_KW)[1])
+
+
+def single_halo_configs(dev, steps: int = 3, warmup: int = 2) -> dict:
+    """Throughput of the stage on the single-halo workloads: the 131072-particle
+    NFW halo (fixed 128^3 mesh, Gaussian 2 cells), the 5e7-particle cluster
+    (512^3, 2 cells) and the 1e7-particle Gaussian mixture (256^3, 1.5 cells),
+    inputs resident, CUDA-event time per step; the first also through the plain
+    FP64 stage."""
+    import torch
+
+    from galaxyfinder_b200 import _lib, batch, synth
+    res = {}
+    for name, make, nmesh, rg in (("single halo 131072, 128^3", synth.config1, 128, 2.0),
+                                  ("cluster 5e7, 512^3", synth.config3, 512, 2.0),
+                                  ("gaussian mixture 1e7, 256^3", synth.config4, 256, 1.5)):
+        hb = make()
+        ctx = batch.Context(dev.index or 0)
+        db = batch.DeviceBatch.from_halobatch(hb, device=dev)
+        rule = batch.mesh_rule(mode=_lib.MESH_FIXED, nfixed=nmesh, rg=rg, rg_in_cells=True)
+        entry = {"particles": int(hb.n)}
+        for label, cfg in (("batched_fp32", batch.stage_config(mesh=rule, knn_k=K_NEIGH)),
+                           ("plain_fp64", batch.stage_config(mesh=rule, knn_k=K_NEIGH, plain_fp64=True))):
+            if label == "plain_fp64" and hb.n > 1_000_000:
+                continue
+            out = batch.StageBuffers(hb.n, K_NEIGH, dev)
+            for _ in range(warmup):
+                batch.stage_run(ctx, db, cfg, out)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ctx.stream)
+            for _ in range(steps):
+                batch.stage_run(ctx, db, cfg, out)
+            e1.record(ctx.stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            _, st = batch.stage_run(ctx, db, cfg, out, stats=True)
+            entry[label] = {"value": hb.n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+                            "phases_ms": {k[3:]: st[k] for k in st if k.startswith("ms_") and k != "ms_pad"}}
+            del out
+        if "plain_fp64" in entry:
+            entry["batched_over_plain"] = entry["batched_fp32"]["value"] / entry["plain_fp64"]["value"]
+        res[name] = entry
+        ctx.close()
+        del db, hb
+        torch.cuda.empty_cache()
+    return res
 
 
 def workload_config(args, hb, world: int, mesh_cells: int) -> dict:
@@ -576,21 +624,31 @@ def main():
     pipe.close()
     del pipe
 
-    # ---- plain GPU path: one halo per gf_stage_run call, same kernels,
-    # inputs resident (the batching's own gain), over the whole catalogue
-    views = batch.HaloViews(db, out, K_NEIGH, hb.pstart)
-    views.run(ctx, cfg, halos=range(min(64, hb.nhalo)))
-    torch.cuda.synchronize()
-    barrier()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    views.run(ctx, cfg)
-    g1.record(stream)
-    torch.cuda.synchronize()
-    plain_ms = max_over_ranks(g0.elapsed_time(g1))
+    # ---- plain GPU path: every phase in FP64 (plain_fp64), one halo per
+    # gf_stage_run call, inputs resident; and, for the batching's own gain,
+    # the same FP32 kernels one halo per call
+    def one_halo_per_call(c):
+        views = batch.HaloViews(db, out, K_NEIGH, hb.pstart)
+        views.run(ctx, c, halos=range(min(64, hb.nhalo)))
+        torch.cuda.synchronize()
+        barrier()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        views.run(ctx, c)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(g0.elapsed_time(g1))
+
+    cfg64 = batch.stage_config(mesh=mesh_rule, knn_k=K_NEIGH, plain_fp64=True)
+    plain_ms = one_halo_per_call(cfg64)
+    plain32_ms = one_halo_per_call(cfg)
+    headline = pipe_res["resident"]["value"]
     plain = {"value": total_particles / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
-             "path": "one halo per gf_stage_run call (device-resident inputs, same kernels)",
-             "batched_over_plain": value / (total_particles / (plain_ms / 1e3))}
+             "path": "plain FP64 stage: every phase in FP64 (exact FP64 kNN, FP64 TSC/FFT/findDen meshes, "
+                     "FP64 Barnes-Hut terms), one halo per gf_stage_run call, device-resident inputs",
+             "batched_over_plain": headline / (total_particles / (plain_ms / 1e3)),
+             "fp32_one_halo_per_call": {"value": total_particles / (plain32_ms / 1e3), "ms_per_step": plain32_ms,
+                                        "batched_over_it": headline / (total_particles / (plain32_ms / 1e3))}}
 
     # ---- roofline of the dominant kernel
     pk = peaks()
@@ -603,10 +661,16 @@ def main():
     # and writes the mesh once; smoothing reads and writes the mesh twice
     # (16 B per cell floor); findDen reads FP64 x, y, z, the mesh, writes a float
     # (its 27-cell stencils re-read the mesh the smoothing has just written,
-    # shared between neighbouring particles: working set, not counted)
+    # shared between neighbouring particles: working set, not counted).
+    # Meshes of 64^3 never reach device memory: the on-chip kernel (in the
+    # smoothing phase) reads FP64 x, y, z, m and the type of their particles
+    # for the deposit, x, y, z again for the interpolation, and writes a float
+    dev_cells = st.get("mesh_cells_device", cells)
+    n_chip = st.get("onchip_particles", 0)
+    n_dev = n - n_chip
     alg = {"recentre": 52 * n, "tree": 0, "knn": (16 + 4 * K_NEIGH + 4) * n,
-           "tsc": 32 * n + 4 * cells, "smooth": 16 * cells, "findden": 28 * n,
-           "potential": 0}
+           "tsc": 32 * n_dev + 4 * dev_cells, "smooth": 16 * dev_cells + 64 * n_chip,
+           "findden": 28 * n_dev, "potential": 0}
     # the whole stage's algorithmic bytes per step against HBM, for the
     # batched (pipelined and single-stream) and plain paths
     stage_bytes = float(sum(alg.values()))
@@ -662,6 +726,8 @@ def main():
         "config": workload_config(args, hb, world, int(cells)),
         "pipeline": f"{nchunks} halo chunks on their own streams and host threads",
         "tree_nodes": int(st["nnode"]),
+        "meshes": {"cells_planned": int(cells), "cells_in_device_memory": int(dev_cells),
+                   "onchip_meshes": int(st.get("onchip_meshes", 0)), "onchip_particles": int(n_chip)},
         "e2e": {"value": pipe_res["e2e"]["value"], "unit": UNIT, "h2d_bytes_per_step": pipe_h2d,
                 "d2h_bytes_per_step": pipe_d2h, "ms_per_step": pipe_res["e2e"]["ms_per_step"],
                 "path": "PipelinedStage.run_e2e(K): pinned host inputs in, all outputs back to pinned host, "
@@ -708,6 +774,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_accuracy:
         halos = accuracy_sample(hb)
         line["accuracy"] = accuracy_check(ctx, db, cfg, hb, mesh_rule, halos)
+    if rank == 0 and world == 1 and args.configs:
+        line["single_halo_workloads"] = single_halo_configs(dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -745,7 +745,8 @@ knn_bucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_
 // k-th place, duplicate positions) goes to a device list that knn_kernel
 // then serves exactly.  Output rows and densities are written by the warp one
 // query at a time (coalesced), in the arithmetic of knn_kernel.
-constexpr int kFBucketWarpBytes = 32 * 32 * 8 + 32 * (int)sizeof(KnnNode) + 32 * 16 + 32 * 4;
+constexpr int kFBucketWarpBytes = 32 * 32 * 8 + 32 * (int)sizeof(KnnNode) + 32 * 16 + 32 * 4 +
+                                  32 * GF_KNNB_QUEUE * 8;
 
 __device__ __forceinline__ uint64_t pack_key(float f, int id) {
     return ((uint64_t)__float_as_uint(f) << 32) | (uint32_t)id;
@@ -790,6 +791,11 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
     int *win_w = reinterpret_cast<int *>(win);
     const int *nodes_w = reinterpret_cast<const int *>(nodes);
     uint64_t *K = KH + lane;  // this lane's heap column
+    // with GF_KNNB_QUEUE, survivors of the tile filter wait in the lane's
+    // queue column and the warp inserts all lanes' queues together, so the
+    // lanes sift in the same steps instead of one tile's survivors at a time
+    uint64_t *QK = reinterpret_cast<uint64_t *>(cid + 32) + lane;
+    int qn = 0;
     // work counters: node tests, particle tests, heap insertions (per lane),
     // warp-wide insertion steps, queries sent to the exact kernel
     unsigned long long ctr[5] = {0, 0, 0, 0, 0};
@@ -842,6 +848,23 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                 }
                 bf = key_f(rk);
             }
+            // every lane inserts its queued survivors
+            auto flush_queue = [&]() {
+                for (int u = 0; u < qn; u++) {
+                    const uint64_t key = QK[32 * u];
+                    if (key < rk) {
+                        frej = fminf(frej, bf);  // the evicted root
+                        kheap_sift_down(K, 0, kk, key);
+                        rk = K[0];
+                        bf = key_f(rk);
+                        if (COUNT) ctr[2]++;
+                    } else {
+                        frej = fminf(frej, key_f(key));
+                    }
+                }
+                qn = 0;
+            };
+            (void)flush_queue;
             // ---- the smallest subtree holding [qa, qb]
             int c = owner[qa];
             KnnNode C = nodes[c];
@@ -915,6 +938,24 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                             ctr[3] += __reduce_max_sync(0xffffffffu, (unsigned)__popc(pass));
                         }
                         // insert the survivors (each lane its own)
+#if GF_KNNB_QUEUE
+                        while (true) {
+                            while (pass && qn < GF_KNNB_QUEUE) {
+                                const int t = __ffs(pass) - 1;
+                                pass &= pass - 1;
+                                const float f = f_d2_fma(Q, cpos[t]);
+                                const uint64_t key = pack_key(f, cid[t]);
+                                if (key < rk) {
+                                    QK[32 * qn] = key;
+                                    qn++;
+                                } else {
+                                    frej = fminf(frej, f);
+                                }
+                            }
+                            if (!__any_sync(0xffffffffu, pass != 0u)) break;
+                            flush_queue();  // a lane's queue is full
+                        }
+#else
                         while (pass) {
                             const int t = __ffs(pass) - 1;
                             pass &= pass - 1;
@@ -930,9 +971,13 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                                 frej = fminf(frej, f);
                             }
                         }
+#endif
                     }
                     i++;
                 }
+#if GF_KNNB_QUEUE
+                flush_queue();  // the bound is current before the stopping test
+#endif
                 // distance from the query to the outside of C's box (exact
                 // differences of floats, squared in double)
                 const double dbx = fmin((double)Q.x - (double)C.lo[0], (double)C.hi[0] - (double)Q.x);

@@ -40,8 +40,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include "gf_fp64.cuh"
 #include "gf_ref_types.h"
-#include "gf_tree.cuh"
 
 namespace gf {
 
@@ -52,185 +52,6 @@ static_assert(sizeof(TStruct) == 176, "TStruct layout (tree.h:79-91)");
 static_assert(sizeof(particle) == 40, "particle layout (tree.h:145-149)");
 
 constexpr int kMaxNear = 32;  // MAX_NUM_NEAR, tree.h:20
-
-// FP64 moments and box of one preorder node, over its particles.
-struct RefNode {
-    double com[3];
-    double mass;
-    double dist2;   // max |x - com|^2
-    double q[6];    // xx, yy, zz, xy, xz, yz about the com
-    double lo[3], hi[3];
-};
-
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ double warp_max(double v) {
-    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ __forceinline__ double warp_min(double v) {
-    for (int o = 16; o; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// x, y, z, m of the tree's particles gathered into tree order.
-// and the index into the caller's particle array of each tree position.
-__global__ void gather_tree_order(int64_t n, const int32_t *__restrict__ perm,
-                                  const double *__restrict__ x, const double *__restrict__ y,
-                                  const double *__restrict__ z, const float *__restrict__ m,
-                                  const int32_t *__restrict__ set, double4 *__restrict__ out,
-                                  int32_t *__restrict__ tidx) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t p = perm[t];
-        out[t] = make_double4(x[p], y[p], z[p], (double)m[p]);
-        tidx[t] = set[p];
-    }
-}
-
-// A warp per node: mass and centre of mass (divide_node, ost.c:545-555:
-// float masses summed in double), then size and second moments about it.
-__global__ void ref_node_kernel(int32_t nnode, const KnnNode *__restrict__ knn,
-                                const double4 *__restrict__ tp, RefNode *__restrict__ out) {
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nnode; i += warps) {
-        const int a = knn[i].lstart, b = a + knn[i].count;
-        double m = 0, sx = 0, sy = 0, sz = 0;
-        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (int j = a + lane; j < b; j += 32) {
-            const double4 p = tp[j];
-            m += p.w;
-            sx += p.w * p.x;
-            sy += p.w * p.y;
-            sz += p.w * p.z;
-            lo[0] = fmin(lo[0], p.x); hi[0] = fmax(hi[0], p.x);
-            lo[1] = fmin(lo[1], p.y); hi[1] = fmax(hi[1], p.y);
-            lo[2] = fmin(lo[2], p.z); hi[2] = fmax(hi[2], p.z);
-        }
-        m = warp_sum(m);
-        sx = warp_sum(sx);
-        sy = warp_sum(sy);
-        sz = warp_sum(sz);
-        for (int c = 0; c < 3; c++) {
-            lo[c] = warp_min(lo[c]);
-            hi[c] = warp_max(hi[c]);
-        }
-        const double cx = sx / m, cy = sy / m, cz = sz / m;
-        double d2 = 0, q[6] = {0, 0, 0, 0, 0, 0};
-        for (int j = a + lane; j < b; j += 32) {
-            const double4 p = tp[j];
-            const double dx = p.x - cx, dy = p.y - cy, dz = p.z - cz;
-            d2 = fmax(d2, dx * dx + dy * dy + dz * dz);
-            q[0] += p.w * dx * dx;
-            q[1] += p.w * dy * dy;
-            q[2] += p.w * dz * dz;
-            q[3] += p.w * dx * dy;
-            q[4] += p.w * dx * dz;
-            q[5] += p.w * dy * dz;
-        }
-        d2 = warp_max(d2);
-        for (int c = 0; c < 6; c++) q[c] = warp_sum(q[c]);
-        if (lane == 0) {
-            RefNode r;
-            r.com[0] = cx;
-            r.com[1] = cy;
-            r.com[2] = cz;
-            r.mass = m;
-            r.dist2 = d2;
-            for (int c = 0; c < 6; c++) r.q[c] = q[c];
-            for (int c = 0; c < 3; c++) {
-                r.lo[c] = lo[c];
-                r.hi[c] = hi[c];
-            }
-            out[i] = r;
-        }
-    }
-}
-
-// (d2, index) order of the neighbour lists.
-__device__ __forceinline__ bool nb_less(double d2a, int32_t ia, double d2b, int32_t ib) {
-    return d2a < d2b || (d2a == d2b && ia < ib);
-}
-
-// Exact k nearest (k <= 32) of each query point among the tree's particles, a
-// warp per query: lane j keeps the j-th nearest; the walk visits the preorder
-// nodes, skipping a subtree whose FP64 box is farther than the k-th distance.
-// Particle distances are the reference's (dx*dx + dy*dy) + dz*dz in FP64.
-__global__ void knn64_kernel(int64_t nq, const double *__restrict__ qx, const double *__restrict__ qy,
-                             const double *__restrict__ qz, int k, int32_t root, int32_t rend,
-                             const KnnNode *__restrict__ knn, const RefNode *__restrict__ rn,
-                             const double4 *__restrict__ tp, const int32_t *__restrict__ tidx,
-                             int32_t *__restrict__ out_idx, double *__restrict__ out_d2,
-                             int32_t *__restrict__ out_n) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t q = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; q < nq; q += warps) {
-        const double px = qx[q], py = qy[q], pz = qz[q];
-        double my_d2 = INFINITY;  // lane j: j-th nearest so far
-        int32_t my_i = INT32_MAX;
-        int filled = 0;
-        double kth = INFINITY;
-        int32_t kth_i = INT32_MAX;
-        int i = root;
-        while (i < rend) {
-            const KnnNode nd = knn[i];
-            if (filled == k) {
-                const RefNode &r = rn[i];
-                const double dx = fmax(fmax(r.lo[0] - px, px - r.hi[0]), 0.0);
-                const double dy = fmax(fmax(r.lo[1] - py, py - r.hi[1]), 0.0);
-                const double dz = fmax(fmax(r.lo[2] - pz, pz - r.hi[2]), 0.0);
-                if ((dx * dx + dy * dy) + dz * dz > kth) {  // nothing inside can enter the list
-                    i = nd.skip;
-                    continue;
-                }
-            }
-            for (int c = nd.lstart; c < nd.lstart + nd.lcount; c += 32) {
-                const int j = c + lane;
-                double d2 = INFINITY;
-                int32_t id = INT32_MAX;
-                if (j < nd.lstart + nd.lcount) {
-                    const double4 s = tp[j];
-                    const double tx = px - s.x, ty = py - s.y, tz = pz - s.z;
-                    d2 = tx * tx + ty * ty + tz * tz;
-                    id = tidx[j];
-                }
-                unsigned cand = __ballot_sync(0xffffffffu, j < nd.lstart + nd.lcount &&
-                                                               (filled < k || nb_less(d2, id, kth, kth_i)));
-                while (cand) {
-                    const int src = __ffs(cand) - 1;
-                    cand &= cand - 1;
-                    const double cd = __shfl_sync(0xffffffffu, d2, src);
-                    const int32_t ci = __shfl_sync(0xffffffffu, id, src);
-                    if (filled == k && !nb_less(cd, ci, kth, kth_i)) continue;
-                    // position of the candidate: entries before it
-                    const unsigned before = __ballot_sync(0xffffffffu, lane < filled && nb_less(my_d2, my_i, cd, ci));
-                    const int pos = __popc(before);
-                    const double up_d2 = __shfl_up_sync(0xffffffffu, my_d2, 1);
-                    const int32_t up_i = __shfl_up_sync(0xffffffffu, my_i, 1);
-                    if (lane == pos) {
-                        my_d2 = cd;
-                        my_i = ci;
-                    } else if (lane > pos) {
-                        my_d2 = up_d2;
-                        my_i = up_i;
-                    }
-                    if (filled < k) filled++;
-                    kth = __shfl_sync(0xffffffffu, my_d2, k - 1);
-                    kth_i = __shfl_sync(0xffffffffu, my_i, k - 1);
-                }
-            }
-            i++;  // preorder: the first child, or past this node when it has none
-        }
-        if (lane < filled) {
-            out_idx[q * k + lane] = my_i;
-            out_d2[q * k + lane] = my_d2;
-        }
-        if (lane == 0) out_n[q] = filled;
-    }
-}
 
 __global__ void pack_f4(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
                         const double *__restrict__ z, const float *__restrict__ m, float4 *__restrict__ out) {
@@ -360,7 +181,8 @@ int build_device_tree(State &S, Entry *e, float theta2) {
     GF_TRY(S.dpos.reserve((size_t)n * sizeof(double4) + (size_t)n * sizeof(int32_t) + 512));
     double4 *tp = S.dpos.as<double4>();
     int32_t *tidx = reinterpret_cast<int32_t *>(tp + n);
-    gather_tree_order<<<grid_for(n, 256), 256, 0, ctx->stream>>>(n, t.perm, dx, dy, dz, dm, dset, tp, tidx);
+    gather_tree_order<<<grid_for(n, 256), 256, 0, ctx->stream>>>(n, t.perm, dx, dy, dz, dm, nullptr, dset,
+                                                                   tp, tidx);
     GF_LAUNCH_CHECK();
     GF_TRY(S.dnodes.reserve((size_t)t.nnode * sizeof(RefNode)));
     ref_node_kernel<<<grid_for((int64_t)t.nnode * 32, 256), 256, 0, ctx->stream>>>(
@@ -559,8 +381,8 @@ int run_knn(State &S, Entry *e, int64_t n, const double *qx, const double *qy, c
     const int64_t threads = n * 32;
     knn64_kernel<<<grid_for(threads, 128), 128, 0, ctx->stream>>>(
         n, reinterpret_cast<const double *>(dq), reinterpret_cast<const double *>(dq + qb),
-        reinterpret_cast<const double *>(dq + 2 * qb), k, S.root, S.rend, ctx->last_tree.knn,
-        S.dnodes.as<RefNode>(), S.dpos.as<double4>(), tidx, oi, od, on);
+        reinterpret_cast<const double *>(dq + 2 * qb), nullptr, k, ctx->last_tree.root, ctx->last_tree.rend,
+        ctx->last_tree.knn, S.dnodes.as<RefNode>(), S.dpos.as<double4>(), tidx, nullptr, oi, od, on, nullptr);
     GF_LAUNCH_CHECK();
     GF_CUDA_TRY(cudaMemcpyAsync(h, dout, ob_i + ob_d + ob_n, cudaMemcpyDeviceToHost, ctx->stream));
     GF_TRY(check_device_errors(ctx));

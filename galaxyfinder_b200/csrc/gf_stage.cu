@@ -169,7 +169,7 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         // out in device memory
         for (int32_t h = 0; h < nh; h++) {
             gf_mesh_desc &m = mesh[h];
-            if (!cfg->mesh_device_only && m.nx == kOnChipMesh && m.ny == kOnChipMesh && m.nz == kOnChipMesh) {
+            if (!cfg->mesh_device_only && !cfg->plain_fp64 && m.nx == kOnChipMesh && m.ny == kOnChipMesh && m.nz == kOnChipMesh) {
                 m.ptype = kMeshOnChip;
                 m.off = 0;
                 onchip_halos.push_back(h);
@@ -199,6 +199,29 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
     if (need_tree)
         GF_TRY(build_tree(ctx, nh, n, b->pstart, pos, cfg->theta2, cfg->q5_asbuilt, &ctx->last_tree));
     tm.mark();  // 2
+    if (cfg->plain_fp64) {
+        const double pf = cfg->potentfact != 0.0 ? cfg->potentfact : physics().potentfact;
+        const PotentialParams pp = potential_params(cfg->theta2, cfg->ndirect, pf, cfg->add_bg);
+        float ms4[4] = {0, 0, 0, 0};
+        GF_TRY(stage_plain_fp64(ctx, b, cfg, o, hid, xr, yr, zr, mesh, mesh_dev, cells, pp, st ? ms4 : nullptr));
+        tm.mark();  // 3: the FP64 phases are timed inside
+        int status = check_device_errors(ctx);
+        if (st) {
+            memset(st, 0, sizeof(*st));
+            st->nparticle = n;
+            st->nhalo = nh;
+            st->nnode = need_tree ? ctx->last_tree.nnode : 0;
+            st->mesh_cells = cells;
+            st->mesh_cells_device = cells;
+            st->ms_recentre = tm.ms(0);
+            st->ms_tree = tm.ms(1);
+            st->ms_knn = ms4[0];
+            st->ms_smooth = ms4[1];
+            st->ms_findden = ms4[2];
+            st->ms_potential = ms4[3];
+        }
+        return status;
+    }
     // ---- 3. kNN + SPH density
     if (cfg->knn_k > 0) {
         if (!o->nearindex) {

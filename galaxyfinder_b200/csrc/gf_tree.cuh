@@ -57,6 +57,14 @@ double nfw_rvir(double mvir);
 int potent_device(gf_ctx *ctx, int nend, const Vector3d *r, int snp, const Vector3d *sr,
                   const float *smass, bool self, float **dout, const double **dtargets);
 
+// The whole stage in FP64 (gf_plain64.cu) after recentring and the octree
+// build on ctx: kNN + SPH density, meshes, potential.  ms (optional) receives
+// the kNN, TSC + smoothing, findDen and potential times.
+int stage_plain_fp64(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *o,
+                     const int32_t *hid, const double *xr, const double *yr, const double *zr,
+                     const std::vector<gf_mesh_desc> &mesh, const gf_mesh_desc *mesh_dev, int64_t cells,
+                     const PotentialParams &pp, float *ms);
+
 // Copies the preorder node arrays and particle order to the host (tests).
 int export_tree(gf_ctx *ctx, const TreeView &t, void *knn_host, void *bh_host, float4 *pos_host,
                 int32_t *perm_host, int32_t *root_host, int32_t *rend_host);

@@ -36,7 +36,8 @@ from pathlib import Path
 from . import build as B
 
 TUNE_DIR = B.PKG / "_tune"
-DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
+DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0,
+            "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
             "GF_BH_BLOCK": 128,
             "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
@@ -54,6 +55,7 @@ def stages(group: str):
                               for a in (1, 2) for b in (32, 64)] +
                 [{"GF_KNN_ALGO": 1, "GF_KNNB_BLOCK": 32, "GF_KNNB_ARITY": 4}, {"GF_KNN_ALGO": 0}],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_SEEDS": n} for n in (32, 48, 64, 96)],
+                lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_QUEUE": q} for q in (0, 2, 4, 8)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else
                 [{"GF_KNN_BLOCK": b, "GF_KNN_MINB": minb(b, r)} for b in (128, 256) for r in REGCAPS]]

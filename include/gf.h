@@ -407,7 +407,9 @@ typedef struct gf_stage_config {
     int32_t mesh_device_only; /* 1: every mesh through device memory; 0: 64^3 meshes run
                                  their whole mesh stage in one thread-block cluster's
                                  shared memory */
-    int32_t reserved;
+    int32_t plain_fp64;    /* 1: the plain FP64 stage (every phase in FP64 by straightforward
+                              kernels, meshes in device memory), the baseline the batched
+                              FP32 stage is compared with */
 } gf_stage_config;
 
 typedef struct gf_stage_out {
