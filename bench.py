@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunks", type=int, default=8,
                     help="halo chunks (streams) of the pipelined stage")
+    ap.add_argument("--postprocessing", action="store_true",
+                    help="run only the full post-processing workload (1e5 groups + centre refinement) and "
+                         "print its line")
     ap.add_argument("--configs", action="store_true",
                     help="also time the single-halo workloads (131072-particle halo, 5e7 cluster, 1e7 mixture)")
     ap.add_argument("--no-accuracy", action="store_true",
@@ -349,6 +352,95 @@ def single_halo_configs(dev, steps: int = 3, warmup: int = 2) -> dict:
     return res
 
 
+def postprocessing_workload(dev, steps: int, warmup: int, nchunk: int = 16, block: int = 2000) -> dict:
+    """The full post-processing run: 1e5 FoF groups from the catalogue law on
+    [50, 1e7] particles with 10 % unbound background particles, the batched
+    stage over all of them (halo chunks on their own streams, inputs resident,
+    CUDA-event time), then the gradient-ascent refinement (<= 20 steps of 0.1
+    smoothing length) of the centre of every group's stellar body on its
+    smoothed stellar mesh (64-256^3), all centres of a block of groups in one
+    launch, and the refined centres against GalCenter's search-based ones
+    (GalCenter/find_centers.c:25-104) on a sample of groups."""
+    import torch
+
+    from galaxyfinder_b200 import _lib, batch, centres, synth
+    from oracle.oracle import GalCenterSearch
+    t0 = time.perf_counter()
+    hb = synth.postprocessing_catalogue()
+    gen_s = time.perf_counter() - t0
+    rule = batch.mesh_rule(mode=_lib.MESH_POW2, nmin=64, nmax=256, rg=2.0, rg_in_cells=True)
+    cfg = batch.stage_config(mesh=rule, knn_k=K_NEIGH)
+    pipe = batch.PipelinedStage(hb, cfg, nchunk=nchunk, device=dev.index or 0, k=K_NEIGH)
+    pipe.run_resident(max(warmup, 1))
+    torch.cuda.synchronize()
+    p0, p1 = pipe.run_resident(steps)
+    torch.cuda.synchronize()
+    stage_ms = p0.elapsed_time(p1) / steps
+    pipe.close()
+    del pipe
+    torch.cuda.empty_cache()
+    # one galaxy per group with >= 30 stars: start at its stellar centre of mass
+    n = halo_counts(hb)
+    ctx = batch.Context(dev.index or 0)
+    srule = batch.mesh_rule(mode=_lib.MESH_POW2, nmin=64, nmax=256, rg=2.0, rg_in_cells=True,
+                            ptype=_lib.TYPE_STAR)
+    refined = {}
+    t0 = time.perf_counter()
+    ngal = moved = 0
+    for h0 in range(0, hb.nhalo, block):
+        h1 = min(hb.nhalo, h0 + block)
+        a, b = int(hb.pstart[h0]), int(hb.pstart[h1])
+        sl = slice(a, b)
+        ps = hb.pstart[h0:h1 + 1] - a
+        starts, halo_of = [], []
+        for h in range(h0, h1):
+            p, ha, hb_ = recentred_halo(hb, h)
+            st = hb.type[ha:hb_] == 1
+            if st.sum() < 30:
+                continue
+            w = hb.mass[ha:hb_][st]
+            c = (p[st] * w[:, None]).sum(0) / w.sum()
+            off = np.array([hb.x[ha], hb.y[ha], hb.z[ha]]) - p[0]  # recentred -> box coordinates
+            starts.append(np.mod(c + off, 100.0))
+            halo_of.append(h - h0)
+        if not starts:
+            continue
+        cen, rho, moves, aux = centres.refine_centres(ctx, hb.x[sl], hb.y[sl], hb.z[sl], hb.mass[sl],
+                                                      hb.type[sl], ps, np.array(starts),
+                                                      np.array(halo_of, np.int32), rule=srule)
+        torch.cuda.synchronize()
+        for i, hl in enumerate(halo_of):
+            refined[h0 + hl] = (cen[i], float(aux["mesh"][hl]["rg"]))
+        ngal += len(starts)
+        moved += int(np.sum(moves > 0))
+        del aux
+    centre_s = time.perf_counter() - t0
+    # against GalCenter's search on a sample of groups of up to 1e5 particles
+    gc = GalCenterSearch()
+    rng = np.random.default_rng(3)
+    cand = [h for h in refined if n[h] <= 100_000]
+    offs = []
+    for h in rng.choice(cand, min(48, len(cand)), replace=False):
+        a, b = int(hb.pstart[h]), int(hb.pstart[h + 1])
+        g, _ = gc.find_centers(hb.x[a:b], hb.y[a:b], hb.z[a:b], hb.mass[a:b], hb.type[a:b])
+        c, rg = refined[int(h)]
+        d = c - g[:3]
+        d -= 100.0 * np.round(d / 100.0)
+        offs.append(np.linalg.norm(d) / rg)
+    ctx.close()
+    offs = np.array(offs)
+    return {"particles": int(hb.n), "groups": int(hb.nhalo), "generation_s": gen_s,
+            "stage": {"value": hb.n / (stage_ms / 1e3), "unit": UNIT, "ms_per_step": stage_ms,
+                      "path": f"PipelinedStage, {nchunk} halo chunks, inputs resident"},
+            "centres": {"galaxies": ngal, "moved": moved, "seconds": centre_s,
+                        "path": "stellar TSC + smoothing (64-256^3) per block of 2000 groups, all centres of a "
+                                "block in one gf_refine_centres launch (<= 20 steps of 0.1 R_G); seconds include "
+                                "the host-side recentring and mesh planning",
+                        "offset_vs_galcenter_over_rg": {"sample": int(len(offs)),
+                                                        "median": float(np.median(offs)) if len(offs) else None,
+                                                        "p90": float(np.quantile(offs, 0.9)) if len(offs) else None}}}
+
+
 def workload_config(args, hb, world: int, mesh_cells: int) -> dict:
     """The `config` object of both arms' JSON lines."""
     return {"workload": f"batched catalogue, {args.nhalo} FoF halos per GPU, N_p ~ N^-1.9 on [100, 2e6], "
@@ -517,6 +609,18 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.postprocessing:
+        res = postprocessing_workload(dev, args.steps, args.warmup)
+        line = dict(base)
+        line.update({"value": res["stage"]["value"], "ms_per_step": res["stage"]["ms_per_step"],
+                     "config": {"workload": "full post-processing run: 1e5 FoF groups, N_p ~ N^-1.9 on "
+                                            "[50, 1e7], 10% unbound background, k=32, per-group TSC mesh "
+                                            "64-256^3, Gaussian 2 cells, Barnes-Hut theta2=0.5, then centre "
+                                            "refinement", "particles": res["particles"]},
+                     "postprocessing": res})
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     hb = synth.catalogue(seed=synth.SEED_BASE + 2 + 1000 * rank, nhalo=args.nhalo)
     ctx = batch.Context(local)
     db = batch.DeviceBatch.from_halobatch(hb, device=dev)

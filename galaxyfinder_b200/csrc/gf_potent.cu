@@ -81,9 +81,7 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
             P = tpos[t];
         }
         const double px = P.x, py = P.y, pz = P.z;
-        // four compensated accumulators: the particle terms of a leaf go to
-        // them in turn, so four independent dependency chains are in flight
-        Kahan acc[4];
+        Kahan acc;
         while (true) {
             const int i = (int)__reduce_min_sync(0xffffffffu, (unsigned)my);
             if (i == INT_MAX) break;
@@ -97,26 +95,18 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
                                             __dmul_rn(dz, dz));
                 if (always_open || d2 < nd.open_r2) {
                     const int l1 = nd.lstart + nd.lcount;
-                    // ost.c:186-191: float offsets of the two positions.  For
-                    // float inputs the FP32 difference is the correctly
-                    // rounded exact difference, i.e. the same bits as
-                    // rounding the FP64 difference.
-                    auto term = [&](const float4 &S) {
+                    for (int j = nd.lstart; j < l1; j++) {
+                        const float4 S = spos[j];
+                        // ost.c:186-191: float offsets of the two positions.  For
+                        // float inputs the FP32 difference is the correctly
+                        // rounded exact difference, i.e. the same bits as
+                        // rounding the FP64 difference.
                         const float fx = P.x - S.x;
                         const float fy = P.y - S.y;
                         const float fz = P.z - S.z;
                         const float r2 = fx * fx + fy * fy + fz * fz;
-                        return r2 > 0.f ? -S.w * rsqrtf(r2) : 0.f;
-                    };
-                    int j = nd.lstart;
-                    for (; j + 4 <= l1; j += 4) {  // loads first, then four independent sums
-                        const float4 S0 = spos[j], S1 = spos[j + 1], S2 = spos[j + 2], S3 = spos[j + 3];
-                        acc[0].add(term(S0));
-                        acc[1].add(term(S1));
-                        acc[2].add(term(S2));
-                        acc[3].add(term(S3));
+                        if (r2 > 0.f) acc.add(-S.w * rsqrtf(r2));
                     }
-                    for (int u = 0; j < l1; j++, u++) acc[u].add(term(spos[j]));
                     npp += nd.lcount;
                     my = i + 1;
                 } else {
@@ -127,7 +117,7 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
                     const float inv3 = inv * inv2;
                     const float qxy = nd.q[0] * fx * fx + nd.q[1] * fy * fy + nd.q[2] * fz * fz +
                                       2.f * (nd.q[3] * fx * fy + nd.q[4] * fx * fz + nd.q[5] * fy * fz);
-                    acc[npc & 3].add(-nd.mass * inv + 0.5f * nd.trq * inv3 - 1.5f * qxy * inv3 * inv2);
+                    acc.add(-nd.mass * inv + 0.5f * nd.trq * inv3 - 1.5f * qxy * inv3 * inv2);
                     npc++;
                     my = nd.skip;
                 }
@@ -136,9 +126,7 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
         }
         if (valid) {
             const int64_t o = tout ? tout[t] : t;
-            // the four compensated sums combined in FP64, rounded once
-            const float phi = (float)(((double)acc[0].s - (double)acc[0].c) + ((double)acc[1].s - (double)acc[1].c) +
-                                      (((double)acc[2].s - (double)acc[2].c) + ((double)acc[3].s - (double)acc[3].c)));
+            const float phi = acc.s + (-acc.c);
             if (raw) raw[o] = phi;
             if (out) {
                 double e = pp.potentfact != 0.0 ? (double)phi * pp.potentfact : (double)phi;

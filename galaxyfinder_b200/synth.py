@@ -273,6 +273,35 @@ def catalogue(seed: int = SEED_BASE + 2, nhalo: int = 4096, nmin: int = 100,
     return _finish(P, M, T, rng, {"config": 2, "seed": seed, "nhalo": nhalo})
 
 
+def postprocessing_catalogue(seed: int = SEED_BASE + 5, nhalo: int = 100_000, nmin: int = 50,
+                             nmax: int = 10_000_000, background_frac: float = 0.1,
+                             star_frac: float = 0.2) -> HaloBatch:
+    """The full post-processing workload: nhalo halos from the catalogue law
+    (N_p ~ N^-1.9 on [nmin, nmax], NFW with subhalos and stars, as
+    `catalogue`), each FoF group also holding background_frac x N_p unbound
+    DM particles spread uniformly over its r200 sphere (the unbound
+    background of the groups).  The expected total is about 1.1e8 group
+    particles for the default law; the realised count is in pstart[-1]."""
+    rng = np.random.default_rng(seed)
+    counts = powerlaw_counts(rng, nhalo, nmin, nmax)
+    P, M, T = [], [], []
+    for npart in counts:
+        p, m, t = _catalogue_halo(rng, int(npart), star_frac, rng.random() < 0.05)
+        nb = int(round(background_frac * npart))
+        if nb:
+            # uniform in the r200 sphere about the group's centre of mass
+            r200 = r200_of_mass(float(m.sum()))
+            ctr = p[np.argmin(np.abs(p - np.median(p, 0)).sum(1))]
+            rb = r200 * rng.random(nb) ** (1.0 / 3.0)
+            pb = _wrap(ctr[None, :] + rb[:, None] * _directions(rng, nb))
+            p = np.concatenate([p, pb])
+            m = np.concatenate([m, np.full(nb, DM_MASS)])
+            t = np.concatenate([t, np.full(nb, TYPE_DM, np.int32)])
+        P.append(p); M.append(m); T.append(t)
+    return _finish(P, M, T, rng, {"config": 5, "seed": seed, "nhalo": nhalo,
+                                  "background_frac": background_frac})
+
+
 def gaussian_blob(seed: int, n: int, sigma: float = 0.05, centre=(50.0, 50.0, 50.0),
                   mass: float = DM_MASS) -> HaloBatch:
     """Small isotropic Gaussian halo used by unit tests."""
