@@ -116,7 +116,7 @@ class StageConfig(ctypes.Structure):
         ("do_mesh", ctypes.c_int32), ("do_potential", ctypes.c_int32), ("ndirect", ctypes.c_int32),
         ("theta2", ctypes.c_float), ("add_bg", ctypes.c_int32), ("q5_asbuilt", ctypes.c_int32),
         ("count_work", ctypes.c_int32), ("potentfact", ctypes.c_double),
-        ("mesh_device_only", ctypes.c_int32), ("plain_fp64", ctypes.c_int32),
+        ("mesh_onchip", ctypes.c_int32), ("plain_fp64", ctypes.c_int32),
     ]
 
 

@@ -147,16 +147,16 @@ def self_potential(ctx: Context, pstart, pos4, theta2=0.5, ndirect=0, potentfact
 
 def stage_config(mesh: MeshRule | None = None, box=100.0, knn_k=32, do_mesh=True,
                  do_potential=True, ndirect=100, theta2=0.5, add_bg=True, q5_asbuilt=False,
-                 potentfact=0.0, count_work=False, mesh_device_only=False,
+                 potentfact=0.0, count_work=False, mesh_onchip=False,
                  plain_fp64=False) -> _lib.StageConfig:
-    """mesh_device_only: run every mesh through device memory instead of
-    keeping 64^3 meshes on chip (one thread-block cluster per mesh).
+    """mesh_onchip: keep 64^3 meshes on chip (one thread-block cluster per
+    mesh) instead of in device memory.
     plain_fp64: the plain FP64 stage (every phase in FP64)."""
     if mesh is None:
         mesh = mesh_rule(mode=_lib.MESH_POW2, rg=2.0, rg_in_cells=True)
     return _lib.StageConfig(mesh, box, knn_k, int(do_mesh), int(do_potential), ndirect, theta2,
                             int(add_bg), int(q5_asbuilt), int(count_work), potentfact,
-                            int(mesh_device_only), int(plain_fp64))
+                            int(mesh_onchip), int(plain_fp64))
 
 
 class StageBuffers:

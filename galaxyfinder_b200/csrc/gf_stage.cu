@@ -169,7 +169,7 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         // out in device memory
         for (int32_t h = 0; h < nh; h++) {
             gf_mesh_desc &m = mesh[h];
-            if (!cfg->mesh_device_only && !cfg->plain_fp64 && m.nx == kOnChipMesh && m.ny == kOnChipMesh && m.nz == kOnChipMesh) {
+            if (cfg->mesh_onchip && !cfg->plain_fp64 && m.nx == kOnChipMesh && m.ny == kOnChipMesh && m.nz == kOnChipMesh) {
                 m.ptype = kMeshOnChip;
                 m.off = 0;
                 onchip_halos.push_back(h);

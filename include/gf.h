@@ -404,9 +404,10 @@ typedef struct gf_stage_config {
     int32_t q5_asbuilt;    /* reproduce ost.c:571's y*x in place of y*z */
     int32_t count_work;    /* with stats: also count kNN/potential work (slower) */
     double potentfact;     /* 0: from gf_get_physics() */
-    int32_t mesh_device_only; /* 1: every mesh through device memory; 0: 64^3 meshes run
-                                 their whole mesh stage in one thread-block cluster's
-                                 shared memory */
+    int32_t mesh_onchip;   /* 1: 64^3 meshes run their whole mesh stage (TSC, smoothing,
+                              findDen) in one thread-block cluster's distributed shared
+                              memory; 0: every mesh through device memory (faster on the
+                              benchmark catalogue: 18.2 vs 32.2 ms of smoothing) */
     int32_t plain_fp64;    /* 1: the plain FP64 stage (every phase in FP64 by straightforward
                               kernels, meshes in device memory), the baseline the batched
                               FP32 stage is compared with */

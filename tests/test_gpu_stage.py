@@ -147,8 +147,8 @@ def test_onchip_meshes_match_device_meshes(run):
     hb = run["hb"]
     ctx = batch.Context(0)
     db = batch.DeviceBatch.from_halobatch(hb)
-    on = batch.stage_run(ctx, db, batch.stage_config(knn_k=0, do_potential=False))
-    off = batch.stage_run(ctx, db, batch.stage_config(knn_k=0, do_potential=False, mesh_device_only=True))
+    on = batch.stage_run(ctx, db, batch.stage_config(knn_k=0, do_potential=False, mesh_onchip=True))
+    off = batch.stage_run(ctx, db, batch.stage_config(knn_k=0, do_potential=False))
     torch.cuda.synchronize()
     a, b = on.dens_mesh.cpu().numpy(), off.dens_mesh.cpu().numpy()
     ps = hb.pstart
