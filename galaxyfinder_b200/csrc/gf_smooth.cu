@@ -531,20 +531,34 @@ int launch_onchip(gf_ctx *ctx, const OnChipArgs &a) {
 
 constexpr int kPencils = GF_FFT_PENCILS;  // real pencils per FFT tile (2 per complex pencil)
 
+// Real pencils per tile of an FFT axis of 2^LOGN cells: wider tiles for the
+// short axes, whose tiles are otherwise small (8 KB at 64 cells).
+template <int LOGN>
+struct FftTile {
+    static constexpr int P = LOGN == 6 ? GF_FFT_PENCILS_64 : LOGN == 7 ? GF_FFT_PENCILS_128 : kPencils;
+    static constexpr int NT = (P / 2) * (1 << LOGN) / 8;  // threads per tile
+};
+static_assert(FftTile<9>::NT <= 1024 && FftTile<6>::NT <= 1024 && FftTile<7>::NT <= 1024, "FFT tile threads");
+
+int fft_tile_pencils(int n) {
+    return n == 64 ? FftTile<6>::P : n == 128 ? FftTile<7>::P : kPencils;
+}
+
 template <int AXIS, int LOGN>
-__global__ void __launch_bounds__((kPencils / 2) * (1 << LOGN) / 8)
+__global__ void __launch_bounds__(FftTile<LOGN>::NT)
 smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh, GroupLaunch g,
                   const AxisTable *__restrict__ axes, const float *__restrict__ tables) {
     constexpr int N = 1 << LOGN;
+    constexpr int P = FftTile<LOGN>::P;
     using L = FftLayout<N>;
     extern __shared__ float2 smem[];
-    const SmoothTile t = decode_group_tile<AXIS>(blockIdx.x, g, mesh, kPencils);
+    const SmoothTile t = decode_group_tile<AXIS>(blockIdx.x, g, mesh, P);
     const gf_mesh_desc m = mesh[t.halo];
     const AxisTable at = axes[3 * t.halo + AXIS];
     const int64_t mx = 2 * (m.nx / 2 + 1);
     const int npair = (t.npen + 1) >> 1;
     float2 *b0 = smem;
-    float2 *b1 = smem + (kPencils / 2) * L::SN;
+    float2 *b1 = smem + (P / 2) * L::SN;
     float *fa = reinterpret_cast<float *>(b0);
     // element (pencil p, position s) lives at base + p*pstride + s*sstride;
     // within one tile the offsets fit in 32 bits (axes <= 512, mx*ny < 2^21)
@@ -558,9 +572,9 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
     // All of a thread's loads are issued before any is stored to shared
     // memory (a fixed count per thread, unrolled), so each warp keeps them
     // all in flight.
-    constexpr int NT = (kPencils / 2) * N / 8;  // threads per tile
+    constexpr int NT = FftTile<LOGN>::NT;  // threads per tile
     if (AXIS == 0) {  // rows: consecutive threads walk along a row
-        constexpr int PER = kPencils * N / NT;
+        constexpr int PER = P * N / NT;
         float v[PER];
 #pragma unroll
         for (int r = 0; r < PER; r++) {
@@ -574,17 +588,17 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
             const int p = e >> LOGN, s = e & (N - 1);
             fa[2 * L::at(p >> 1, s) + (p & 1)] = v[r];
         }
-    } else {  // columns: lane = pencil (consecutive x), warps step along the axis
-        constexpr int NW = NT / 32;
-        constexpr int PER = N / NW;
-        const int p = threadIdx.x & 31;
-        const int w = threadIdx.x >> 5;
+    } else {  // columns: consecutive threads take consecutive pencils (x), groups of P step along the axis
+        constexpr int NG = NT / P;
+        constexpr int PER = N / NG;
+        const int p = threadIdx.x % P;
+        const int w = threadIdx.x / P;
         if (p < npen2) {
             float v[PER];
 #pragma unroll
-            for (int r = 0; r < PER; r++) v[r] = p < t.npen ? gsrc[p + (w + r * NW) * sstride] : 0.f;
+            for (int r = 0; r < PER; r++) v[r] = p < t.npen ? gsrc[p + (w + r * NG) * sstride] : 0.f;
 #pragma unroll
-            for (int r = 0; r < PER; r++) fa[2 * L::at(p >> 1, w + r * NW) + (p & 1)] = v[r];
+            for (int r = 0; r < PER; r++) fa[2 * L::at(p >> 1, w + r * NG) + (p & 1)] = v[r];
         }
     }
     __syncthreads();
@@ -600,9 +614,10 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
             if (p < t.npen) gdst[p * pstride + s] = fs[2 * L::at(p >> 1, s) + (p & 1)];
         }
     } else {
-        const int p = threadIdx.x & 31;
+        constexpr int NG = NT / P;
+        const int p = threadIdx.x % P;
         if (p < t.npen) {
-            for (int s = threadIdx.x >> 5; s < N; s += blockDim.x >> 5)
+            for (int s = threadIdx.x / P; s < N; s += NG)
                 gdst[p + s * sstride] = fs[2 * L::at(p >> 1, s) + (p & 1)];
         }
     }
@@ -691,8 +706,8 @@ template <int AXIS, int LOGN>
 int launch_fft(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunch g, int64_t ntiles,
                const AxisTable *axes, const float *tables) {
     constexpr int N = 1 << LOGN;
-    const int threads = (kPencils / 2) * N / 8;
-    const size_t smem = (size_t)2 * (kPencils / 2) * FftLayout<N>::SN * sizeof(float2);
+    const int threads = FftTile<LOGN>::NT;
+    const size_t smem = (size_t)2 * (FftTile<LOGN>::P / 2) * FftLayout<N>::SN * sizeof(float2);
     GF_CUDA_TRY(cudaFuncSetAttribute(smooth_fft_kernel<AXIS, LOGN>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     smooth_fft_kernel<AXIS, LOGN><<<(unsigned)ntiles, threads, smem, ctx->stream>>>(den, mesh_dev, g,
@@ -709,11 +724,11 @@ int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLau
         set_status(GF_ENOTIMPL, "%lld smoothing tiles exceed one launch", (long long)ntiles);
         return GF_ENOTIMPL;
     }
-    if (path_of(n) == PATH_FFT8 && pmax != kPencils) {
-        // the FFT kernel decodes every tile as kPencils pencils: a plan cut
-        // for another width would leave pencils unsmoothed
+    if (path_of(n) == PATH_FFT8 && pmax != fft_tile_pencils(n)) {
+        // the FFT kernel decodes every tile as fft_tile_pencils(n) pencils: a
+        // plan cut for another width would leave pencils unsmoothed
         set_status(GF_EINVAL, "smoothing plan of %d pencils per tile for a %d-cell FFT axis; the "
-                   "kernel was built for %d", pmax, n, kPencils);
+                   "kernel was built for %d", pmax, n, fft_tile_pencils(n));
         return GF_EINVAL;
     }
     switch (path_of(n) == PATH_FFT8 ? ilog2_exact(n) : 0) {
@@ -789,7 +804,7 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
     }
     for (Group &g : groups) {
         if (path_of(g.n) == PATH_FFT8 && g.n == (1 << ilog2_exact(g.n))) {
-            g.pmax = kPencils;
+            g.pmax = fft_tile_pencils(g.n);
         } else {
             int pmax = 32;
             while (pmax > 2 && (size_t)2 * (pmax / 2) * g.n * sizeof(float2) > 200 * 1024) pmax -= 2;
@@ -926,9 +941,9 @@ int smooth_single_build(const gf_mesh_desc &m, unsigned char *blob, size_t cap, 
         double g[kNoAllocMaxAxis], c[kNoAllocMaxAxis];
         write_axis_tables(n, rg_cells, tab + used, g, c);
         used += k;
-        // tiles as smooth_meshes cuts them: kPencils pencils on the FFT path
-        // (the width the FFT kernel decodes), else as many as fit in shared memory
-        int pmax = kPencils;
+        // tiles as smooth_meshes cuts them: the FFT kernel's tile width on the
+        // FFT path, else as many as fit in shared memory
+        int pmax = fft_tile_pencils(n);
         if (path_of(n) != PATH_FFT8) {
             pmax = 32;
             while (pmax > 2 && (size_t)2 * (pmax / 2) * n * sizeof(float2) > 200 * 1024) pmax -= 2;

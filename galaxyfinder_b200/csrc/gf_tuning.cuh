@@ -34,11 +34,20 @@
 #ifndef GF_BH_BLOCK    // threads per block of bh_kernel
 #define GF_BH_BLOCK 128
 #endif
+#ifndef GF_BH_ALGO     // Barnes-Hut walk: 0 terms evaluated in the lockstep walk, 1 queued per lane
+#define GF_BH_ALGO 0
+#endif
 #ifndef GF_BH_MINB
 #define GF_BH_MINB 1
 #endif
 #ifndef GF_FFT_PENCILS // real pencils per shared-memory FFT tile (2 per complex pencil)
 #define GF_FFT_PENCILS 32
+#endif
+#ifndef GF_FFT_PENCILS_64  // real pencils per tile of the 64-cell FFT axes
+#define GF_FFT_PENCILS_64 32
+#endif
+#ifndef GF_FFT_PENCILS_128 // real pencils per tile of the 128-cell FFT axes
+#define GF_FFT_PENCILS_128 32
 #endif
 #ifndef GF_TREE_BLOCK  // threads per block of the per-particle tree-build kernels
 #define GF_TREE_BLOCK 256
@@ -52,5 +61,10 @@ static_assert(GF_KNNB_ARITY == 2 || GF_KNNB_ARITY == 4, "GF_KNNB_ARITY");
 static_assert(GF_KNNB_QUEUE >= 0 && GF_KNNB_QUEUE <= 16, "GF_KNNB_QUEUE");
 static_assert(GF_KNNB_SEEDS >= 32 && GF_KNNB_SEEDS % 2 == 0, "GF_KNNB_SEEDS");
 static_assert(GF_BH_BLOCK % 32 == 0 && GF_BH_BLOCK <= 1024, "GF_BH_BLOCK");
+static_assert(GF_BH_ALGO == 0 || GF_BH_ALGO == 1, "GF_BH_ALGO");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");
+static_assert(GF_FFT_PENCILS_64 >= 32 && GF_FFT_PENCILS_64 <= 128 &&
+                  (GF_FFT_PENCILS_64 & (GF_FFT_PENCILS_64 - 1)) == 0, "GF_FFT_PENCILS_64");
+static_assert(GF_FFT_PENCILS_128 >= 32 && GF_FFT_PENCILS_128 <= 64 &&
+                  (GF_FFT_PENCILS_128 & (GF_FFT_PENCILS_128 - 1)) == 0, "GF_FFT_PENCILS_128");
 static_assert(GF_TREE_BLOCK % 32 == 0 && GF_TREE_BLOCK >= 128 && GF_TREE_BLOCK <= 1024, "GF_TREE_BLOCK");

@@ -38,8 +38,8 @@ from . import build as B
 TUNE_DIR = B.PKG / "_tune"
 DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0,
             "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
-            "GF_BH_BLOCK": 128,
-            "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_TREE_BLOCK": 256}
+            "GF_BH_BLOCK": 128, "GF_BH_ALGO": 0,
+            "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
 
 
@@ -60,10 +60,13 @@ def stages(group: str):
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else
                 [{"GF_KNN_BLOCK": b, "GF_KNN_MINB": minb(b, r)} for b in (128, 256) for r in REGCAPS]]
     if group == "bh":
-        return [lambda base: [{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],
+        return [lambda base: [{"GF_BH_ALGO": a} for a in (0, 1)],
+                lambda base: [{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],
                 lambda base: [{"GF_BH_MINB": minb(base["GF_BH_BLOCK"], r)} for r in REGCAPS]]
     if group == "fft":
-        return [lambda base: [{"GF_FFT_PENCILS": p} for p in (16, 32)]]
+        return [lambda base: [{"GF_FFT_PENCILS": p} for p in (16, 32)],
+                lambda base: [{"GF_FFT_PENCILS_64": p} for p in (32, 64, 128)],
+                lambda base: [{"GF_FFT_PENCILS_128": p} for p in (32, 64)]]
     if group == "tree":
         return [lambda base: [{"GF_TREE_BLOCK": b} for b in (128, 256, 512)]]
     raise ValueError(group)
