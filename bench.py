@@ -839,7 +839,13 @@ def main():
         "pipeline": f"{nchunks} halo chunks on their own streams and host threads",
         "tree_nodes": int(st["nnode"]),
         "meshes": {"cells_planned": int(cells), "cells_in_device_memory": int(dev_cells),
-                   "onchip_meshes": int(st.get("onchip_meshes", 0)), "onchip_particles": int(n_chip)},
+                   "onchip_meshes": int(st.get("onchip_meshes", 0)), "onchip_particles": int(n_chip),
+                   # the smoothing passes skip pencils that are all zero (outside
+                   # the cells the TSC stencils reach) and, on the last pass, the
+                   # columns no findDen stencil reads
+                   "smoothing_pass_cells": int(st.get("mesh_pass_cells", 0)),
+                   "smoothing_pass_fraction": (st.get("mesh_pass_cells", 0) / (3.0 * dev_cells)
+                                               if dev_cells else None)},
         "e2e": {"value": pipe_res["e2e"]["value"], "unit": UNIT, "h2d_bytes_per_step": pipe_h2d,
                 "d2h_bytes_per_step": pipe_d2h, "ms_per_step": pipe_res["e2e"]["ms_per_step"],
                 "path": "PipelinedStage.run_e2e(K): pinned host inputs in, all outputs back to pinned host, "

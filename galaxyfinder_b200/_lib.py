@@ -140,7 +140,7 @@ class StageStats(ctypes.Structure):
         ("knn_candidates", ctypes.c_uint64), ("knn_single_inserts", ctypes.c_uint64),
         ("knn_bitonic_merges", ctypes.c_uint64),
         ("mesh_cells_device", ctypes.c_int64), ("onchip_meshes", ctypes.c_int64),
-        ("onchip_particles", ctypes.c_int64),
+        ("onchip_particles", ctypes.c_int64), ("mesh_pass_cells", ctypes.c_int64),
     ]
 
 

@@ -372,7 +372,7 @@ int gf_ctx_destroy(gf_ctx *c) {
     cudaStreamSynchronize(c->stream);
     c->hid.release();
     c->mesh.release();
-    c->smooth_tiles.release();
+    c->mesh_boxes.release();
     c->smooth_tables.release();
     c->particles.release();
     for (auto &b : c->tmp) b.release();

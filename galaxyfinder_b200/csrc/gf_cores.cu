@@ -259,9 +259,16 @@ int do_lag_find_stellar_core(SimpleBasicParticleType *bp, int np, int numnear, f
     float *dden = ctx->tmp[0].as<float>();
     GF_CUDA_TRY(cudaMemsetAsync(dden, 0, sizeof(float) * (size_t)cells, ctx->stream));
     const double vf = tsc_volfact();
-    GF_TRY(launch_tsc_deposit(ctx, np, dx, dx + n, dx + 2 * n, dx + 3 * n, dtype, nullptr, dmesh, dden, vf));
+    // occupied box: the smoothing skips all-zero pencils (the whole mesh is
+    // still smoothed: the peak scan reads all of it)
+    GF_TRY(ctx->mesh_boxes.reserve(sizeof(int32_t) * kMeshBoxInts));
+    int32_t *boxes = ctx->mesh_boxes.as<int32_t>();
+    GF_TRY(launch_tsc_deposit(ctx, np, dx, dx + n, dx + 2 * n, dx + 3 * n, dtype, nullptr, dmesh, dden, vf,
+                              nullptr, 1, boxes));
     if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, dden, cells, vf));
-    GF_TRY(smooth_meshes(ctx, 1, &m, dmesh, dden));
+    MeshBoxes mb;
+    mb.dev = boxes;
+    GF_TRY(smooth_meshes(ctx, 1, &m, dmesh, dden, nullptr, &mb));
     GF_TRY(launch_find_den(ctx, np, dx, dx + n, dx + 2 * n, nullptr, dmesh, dden, ddens));
 
     // 3. peaks and their core particles

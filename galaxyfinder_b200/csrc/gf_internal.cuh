@@ -127,7 +127,7 @@ struct gf_ctx {
     bool own_stream = false;
     int *d_err = nullptr;  // device error word
     // scratch buffers, named by use
-    gf::DevBuf hid, mesh, smooth_tiles, smooth_tables, particles, tmp[8];
+    gf::DevBuf hid, mesh, mesh_boxes, smooth_tables, particles, tmp[8];
     gf::DevBuf tree[16];
     gf::HostPinned pin[4];
     gf::TreeView last_tree;  // the most recent build_tree() on this context
@@ -146,10 +146,20 @@ int check_device_errors(gf_ctx *ctx);
 int compute_hid(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart, int32_t *hid);
 
 // Mesh helpers implemented in gf_smooth.cu / gf_tsc.cu.
+//
+// Occupied boxes: kMeshBoxInts ints per mesh, the cell ranges (x lo, x hi,
+// y lo, y hi, z lo, z hi) of every TSC stencil deposited into the mesh, then
+// the same ranges over the stencils of every particle of the halo (where
+// findDen reads).  An empty range has lo > hi.  launch_tsc_deposit fills them
+// when given `boxes`; the smoothing then skips the pencils whose input is
+// all zero (exact: a zero pencil filters to zero) and, with `trim_last`, the
+// last pass's pencils outside the evaluation box (the smoothed mesh is then
+// valid only where findDen reads it).
+constexpr int kMeshBoxInts = 12;
 int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
                        const double *mass, const int32_t *type, const int32_t *hid,
                        const gf_mesh_desc *mesh, float *den, double volfact,
-                       const int32_t *order = nullptr);
+                       const int32_t *order = nullptr, int32_t nhalo = 0, int32_t *boxes = nullptr);
 int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
                     const int32_t *hid, const gf_mesh_desc *mesh, const float *den, float *densph,
                     const int32_t *order = nullptr);
@@ -170,8 +180,13 @@ struct OnChipMeshes {
     float volfold = 1.f;                  // 1 or the exact power-of-two volfact
     float *densph = nullptr;              // device, mesh density at every particle of these halos
 };
+struct MeshBoxes {
+    const int32_t *dev = nullptr;  // kMeshBoxInts per mesh, from launch_tsc_deposit
+    bool trim_last = false;        // last pass only over the evaluation box
+};
 int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
-                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip = nullptr);
+                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip = nullptr,
+                  const MeshBoxes *boxes = nullptr);
 
 // Single-mesh smoothing plan in one contiguous byte blob (see gf_smooth.cu):
 // [mesh desc | 3 axis tables | per axis: halo list, tile prefix | tables].

@@ -800,6 +800,8 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
     // warp-wide insertion steps, queries sent to the exact kernel
     unsigned long long ctr[5] = {0, 0, 0, 0, 0};
     const float kInfF = __int_as_float(0x7f800000);
+    const bool vec_out = k % 4 == 0 && ((uintptr_t)nearindex & 15) == 0;
+    (void)vec_out;
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t nbucket = (n + 31) >> 5;
@@ -999,6 +1001,77 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
             // certification threshold: a lower bound of the exact distance^2
             // of every particle not kept
             const double tcert = fmin((double)frej * (1.0 - 2e-6), tbox * (1.0 - 1e-12));
+#if GF_KNNB_LANECERT
+            // ---- every lane certifies and writes its own query
+            if (me) {
+                // heapsort of the lane's column: ascending (float distance, index)
+                for (int e = kk - 1; e > 0; e--) {
+                    const uint64_t last = K[32 * e];
+                    K[32 * e] = K[0];
+                    kheap_sift_down(K, 0, e, last);
+                }
+                // exact FP64 distances in that order; the float of each
+                // replaces the float key (the density needs nothing else)
+                bool sorted = true;
+                double dprev = 0.0;
+                int iprev = -1;
+#pragma unroll 4
+                for (int e = 0; e < kk; e++) {
+                    const int id = (int)(uint32_t)K[32 * e];
+                    const double d = exact_d2(Q, pos_batch[id]);
+                    sorted = sorted && (e == 0 || !key_lt(d, id, dprev, iprev));
+                    K[32 * e] = pack_key((float)d, id);
+                    dprev = d;
+                    iprev = id;
+                }
+                if (!sorted) {
+                    // near-ties ordered differently by the float keys:
+                    // insertion sort by the exact key (recomputed)
+                    for (int e = 1; e < kk; e++) {
+                        const uint64_t v = K[32 * e];
+                        const int vid = (int)(uint32_t)v;
+                        const double vd = exact_d2(Q, pos_batch[vid]);
+                        int f = e;
+                        for (; f > 0; f--) {
+                            const uint64_t u = K[32 * (f - 1)];
+                            const int uid = (int)(uint32_t)u;
+                            if (!key_lt(vd, vid, exact_d2(Q, pos_batch[uid]), uid)) break;
+                            K[32 * f] = u;
+                        }
+                        K[32 * f] = v;
+                    }
+                    dprev = exact_d2(Q, pos_batch[(int)(uint32_t)K[32 * (kk - 1)]]);
+                }
+                if (dprev < tcert) {
+                    int32_t *row = nearindex + (int64_t)myid * k;
+                    if (vec_out) {
+                        for (int j = 0; j < k; j += 4) {
+                            int4 v;
+                            v.x = j < kk ? (int32_t)((int64_t)(uint32_t)K[32 * j] - hs) : -1;
+                            v.y = j + 1 < kk ? (int32_t)((int64_t)(uint32_t)K[32 * (j + 1)] - hs) : -1;
+                            v.z = j + 2 < kk ? (int32_t)((int64_t)(uint32_t)K[32 * (j + 2)] - hs) : -1;
+                            v.w = j + 3 < kk ? (int32_t)((int64_t)(uint32_t)K[32 * (j + 3)] - hs) : -1;
+                            *reinterpret_cast<int4 *>(row + j) = v;
+                        }
+                    } else {
+                        for (int j = 0; j < k; j++)
+                            row[j] = j < kk ? (int32_t)((int64_t)(uint32_t)K[32 * j] - hs) : -1;
+                    }
+                    if (dens) {
+                        // nnost.c:292,415: maxr = sqrtf(maxdist2); W4(sqrtf(d2_j), maxr/2.)
+                        const float neardist = sqrtf((float)dprev);
+                        const float hh = (float)(neardist / 2.);
+                        float rho = 0.f;
+                        for (int j = 0; j < kk; j++) rho += w4(sqrtf(key_f(K[32 * j])), hh);
+                        dens[myid] = rho;
+                    }
+                } else {
+                    redo[atomicAdd(nredo, 1u)] = (int32_t)q;
+                    if (COUNT) ctr[4]++;
+                }
+            }
+            __syncwarp();
+#else
             // ---- transpose the heaps: entry e of lane l moves to slot
             // 32 e + (l ^ e), so that the warp reads one lane's column
             // without bank conflicts
@@ -1040,10 +1113,14 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                 }
             }
             __syncwarp();
+#endif
         }
     }
     if (COUNT && counters) {
-        for (int off = 16; off; off >>= 1) ctr[2] += __shfl_xor_sync(0xffffffffu, ctr[2], off);
+        for (int off = 16; off; off >>= 1) {
+            ctr[2] += __shfl_xor_sync(0xffffffffu, ctr[2], off);
+            if (GF_KNNB_LANECERT) ctr[4] += __shfl_xor_sync(0xffffffffu, ctr[4], off);
+        }
         if (lane == 0) {
             atomicAdd(counters + 0, ctr[0]);
             atomicAdd(counters + 1, ctr[1]);

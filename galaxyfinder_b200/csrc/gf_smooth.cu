@@ -78,6 +78,33 @@ __device__ __forceinline__ SmoothTile decode_group_tile(int64_t b, const GroupLa
     return t;
 }
 
+// Whether a tile's pencils can change the result, from the mesh's occupied
+// boxes (kMeshBoxInts ints: deposit box, then evaluation box; lo > hi when
+// empty).  The passes run along x, then y, then z.  A pencil whose input is
+// all zero filters to zero, so skipping it is exact: along x, the rows
+// (y, z) outside the deposit box are zero; after the x pass every x of an
+// occupied row is set, so along y the columns (x, z) with z outside the
+// deposit box are zero.  Along z every column is set; with trim the pass
+// runs only over the columns (x, y) of the evaluation box.
+template <int AXIS>
+__device__ __forceinline__ bool tile_needed(const SmoothTile &t, const gf_mesh_desc &m,
+                                            const int32_t *__restrict__ box, int trim) {
+    if (AXIS == 0) {
+        const int ylo = box[2], yhi = box[3], zlo = box[4], zhi = box[5];
+        const int r0 = t.base, r1 = t.base + t.npen - 1;  // rows r = y + ny z
+        const int za = r0 / m.ny, zb = r1 / m.ny;
+        for (int zz = max(za, zlo); zz <= min(zb, zhi); zz++) {
+            const int ya = zz == za ? r0 - zz * m.ny : 0;
+            const int yb = zz == zb ? r1 - zz * m.ny : m.ny - 1;
+            if (max(ya, ylo) <= min(yb, yhi)) return true;
+        }
+        return false;
+    }
+    if (AXIS == 1) return t.other >= box[4] && t.other <= box[5];
+    if (!trim) return box[0] <= box[1];  // all zero when nothing was deposited
+    return t.other >= box[8] && t.other <= box[9] && t.base <= box[7] && t.base + t.npen - 1 >= box[6];
+}
+
 constexpr int kThreads = 256;
 
 template <int AXIS>
@@ -92,10 +119,13 @@ template <int AXIS>
 __global__ void __launch_bounds__(kThreads)
 smooth_axis_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh,
                    GroupLaunch g, const AxisTable *__restrict__ axes,
-                   const float *__restrict__ tables, int pmax) {
+                   const float *__restrict__ tables, int pmax, const int32_t *__restrict__ boxes,
+                   int trim) {
     extern __shared__ float2 smem[];
     const SmoothTile t = decode_group_tile<AXIS>(blockIdx.x, g, mesh, pmax);
     const gf_mesh_desc m = mesh[t.halo];
+    // the whole block leaves together (before any barrier)
+    if (boxes && !tile_needed<AXIS>(t, m, boxes + (int64_t)kMeshBoxInts * t.halo, trim)) return;
     const AxisTable at = axes[3 * t.halo + AXIS];
     const int n = at.n;
     const int64_t mx = 2 * (m.nx / 2 + 1);
@@ -547,13 +577,16 @@ int fft_tile_pencils(int n) {
 template <int AXIS, int LOGN>
 __global__ void __launch_bounds__(FftTile<LOGN>::NT)
 smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh, GroupLaunch g,
-                  const AxisTable *__restrict__ axes, const float *__restrict__ tables) {
+                  const AxisTable *__restrict__ axes, const float *__restrict__ tables,
+                  const int32_t *__restrict__ boxes, int trim) {
     constexpr int N = 1 << LOGN;
     constexpr int P = FftTile<LOGN>::P;
     using L = FftLayout<N>;
     extern __shared__ float2 smem[];
     const SmoothTile t = decode_group_tile<AXIS>(blockIdx.x, g, mesh, P);
     const gf_mesh_desc m = mesh[t.halo];
+    // the whole block leaves together (before any barrier)
+    if (boxes && !tile_needed<AXIS>(t, m, boxes + (int64_t)kMeshBoxInts * t.halo, trim)) return;
     const AxisTable at = axes[3 * t.halo + AXIS];
     const int64_t mx = 2 * (m.nx / 2 + 1);
     const int npair = (t.npen + 1) >> 1;
@@ -704,21 +737,22 @@ void append_tables(std::vector<float> &tab, int n, double rg_cells, AxisTable &a
 
 template <int AXIS, int LOGN>
 int launch_fft(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunch g, int64_t ntiles,
-               const AxisTable *axes, const float *tables) {
+               const AxisTable *axes, const float *tables, const int32_t *boxes, int trim) {
     constexpr int N = 1 << LOGN;
     const int threads = FftTile<LOGN>::NT;
     const size_t smem = (size_t)2 * (FftTile<LOGN>::P / 2) * FftLayout<N>::SN * sizeof(float2);
     GF_CUDA_TRY(cudaFuncSetAttribute(smooth_fft_kernel<AXIS, LOGN>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     smooth_fft_kernel<AXIS, LOGN><<<(unsigned)ntiles, threads, smem, ctx->stream>>>(den, mesh_dev, g,
-                                                                                   axes, tables);
+                                                                                   axes, tables, boxes, trim);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }
 
 template <int AXIS>
 int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunch g,
-                 int64_t ntiles, int n, int pmax, const AxisTable *axes, const float *tables) {
+                 int64_t ntiles, int n, int pmax, const AxisTable *axes, const float *tables,
+                 const int32_t *boxes = nullptr, int trim = 0) {
     if (ntiles == 0) return GF_OK;
     if (ntiles > 0x7fffffffLL) {
         set_status(GF_ENOTIMPL, "%lld smoothing tiles exceed one launch", (long long)ntiles);
@@ -732,17 +766,17 @@ int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLau
         return GF_EINVAL;
     }
     switch (path_of(n) == PATH_FFT8 ? ilog2_exact(n) : 0) {
-        case 6: return launch_fft<AXIS, 6>(ctx, den, mesh_dev, g, ntiles, axes, tables);
-        case 7: return launch_fft<AXIS, 7>(ctx, den, mesh_dev, g, ntiles, axes, tables);
-        case 8: return launch_fft<AXIS, 8>(ctx, den, mesh_dev, g, ntiles, axes, tables);
-        case 9: return launch_fft<AXIS, 9>(ctx, den, mesh_dev, g, ntiles, axes, tables);
+        case 6: return launch_fft<AXIS, 6>(ctx, den, mesh_dev, g, ntiles, axes, tables, boxes, trim);
+        case 7: return launch_fft<AXIS, 7>(ctx, den, mesh_dev, g, ntiles, axes, tables, boxes, trim);
+        case 8: return launch_fft<AXIS, 8>(ctx, den, mesh_dev, g, ntiles, axes, tables, boxes, trim);
+        case 9: return launch_fft<AXIS, 9>(ctx, den, mesh_dev, g, ntiles, axes, tables, boxes, trim);
         default: break;
     }
     const size_t smem = (size_t)2 * ((pmax + 1) / 2) * n * sizeof(float2);
     GF_CUDA_TRY(cudaFuncSetAttribute(smooth_axis_kernel<AXIS>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     smooth_axis_kernel<AXIS><<<(unsigned)ntiles, kThreads, smem, ctx->stream>>>(den, mesh_dev, g, axes,
-                                                                                tables, pmax);
+                                                                                tables, pmax, boxes, trim);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }
@@ -750,7 +784,10 @@ int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLau
 }  // namespace
 
 int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
-                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip) {
+                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip,
+                  const MeshBoxes *boxes) {
+    const int32_t *bx = boxes ? boxes->dev : nullptr;
+    const int trim = boxes && boxes->trim_last ? 1 : 0;
     if (nhalo <= 0) return GF_OK;
     const int32_t non_chip = onchip ? onchip->nmesh : 0;  // meshes on chip
     std::vector<AxisTable> axes(3 * (size_t)nhalo);
@@ -860,9 +897,9 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
         gl.tile_start = reinterpret_cast<const int64_t *>(dbuf + off_s[i]);
         gl.ngroup = (int32_t)g.halos.size();
         const int64_t nt = g.start.back();
-        if (g.axis == 0) GF_TRY(launch_group<0>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
-        else if (g.axis == 1) GF_TRY(launch_group<1>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
-        else GF_TRY(launch_group<2>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab));
+        if (g.axis == 0) GF_TRY(launch_group<0>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab, bx, trim));
+        else if (g.axis == 1) GF_TRY(launch_group<1>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab, bx, trim));
+        else GF_TRY(launch_group<2>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab, bx, trim));
     }
     if (non_chip) {
         OnChipArgs a;

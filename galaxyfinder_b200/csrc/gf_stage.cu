@@ -246,7 +246,12 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         // batch order: the deposit's float sums in octree order were faster
         // (2.73 -> 2.34 ms) but put the densest cells of the 5e7-particle
         // cluster 1.04e-5 from an FP64 deposit, past the 1e-5 target
-        GF_TRY(launch_tsc_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, mesh_dev, den, vf));
+        // the occupied boxes let the smoothing skip all-zero pencils, and its
+        // last pass the columns no particle's findDen stencil reads
+        GF_TRY(ctx->mesh_boxes.reserve(sizeof(int32_t) * kMeshBoxInts * (size_t)std::max(nh, 1)));
+        int32_t *boxes = ctx->mesh_boxes.as<int32_t>();
+        GF_TRY(launch_tsc_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, mesh_dev, den, vf, nullptr, nh,
+                                  boxes));
         if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, dev_cells, vf));
         tm.mark();  // 4
         OnChipMeshes oc;
@@ -267,7 +272,10 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
             oc.volfold = (float)vf;
             oc.densph = o->dens_mesh;
         }
-        GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den, &oc));
+        MeshBoxes mb;
+        mb.dev = boxes;
+        mb.trim_last = true;  // den is read only by find_den below
+        GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den, &oc, &mb));
         tm.mark();  // 5
         if (o->dens_mesh)
             GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh,
@@ -300,6 +308,21 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         st->mesh_cells = cells;
         st->mesh_cells_device = dev_cells;
         st->onchip_meshes = (int64_t)onchip_halos.size();
+        if (cfg->do_mesh && dev_cells > 0 && ctx->mesh_boxes.ptr) {
+            // cells of the pencils the three smoothing passes filter, by the
+            // rule of the smoothing's tile test at pencil granularity
+            std::vector<int32_t> bx((size_t)kMeshBoxInts * nh);
+            cudaMemcpy(bx.data(), ctx->mesh_boxes.ptr, bx.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);
+            auto len = [](int32_t lo, int32_t hi) { return hi >= lo ? (int64_t)hi - lo + 1 : 0; };
+            for (int32_t h = 0; h < nh; h++) {
+                const gf_mesh_desc &m = mesh[h];
+                if (m.ptype == kMeshOnChip) continue;
+                const int32_t *q = &bx[(size_t)kMeshBoxInts * h];
+                st->mesh_pass_cells += (int64_t)m.nx * len(q[2], q[3]) * len(q[4], q[5]);  // x pass
+                st->mesh_pass_cells += (int64_t)m.ny * m.nx * len(q[4], q[5]);              // y pass
+                st->mesh_pass_cells += (int64_t)m.nz * len(q[6], q[7]) * len(q[8], q[9]);  // z pass, trimmed
+            }
+        }
         std::vector<int64_t> ps_host;
         if (!onchip_halos.empty()) {
             ps_host.resize((size_t)nh + 1);

@@ -7,11 +7,46 @@
 // the same FP64 positions.  The only difference left in the deposited mesh
 // is the order in which float atomics sum the contributions of different
 // particles to one cell.
+#include <limits.h>
+
+#include <algorithm>
+
 #include "gf_tsc_weights.cuh"
 
 namespace gf {
 
 namespace {
+
+__global__ void box_init_kernel(int32_t *__restrict__ boxes, int64_t nint) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nint; i += (int64_t)gridDim.x * blockDim.x)
+        boxes[i] = (i & 1) ? INT_MIN : INT_MAX;  // empty ranges: lo > hi
+}
+
+// Widens the occupied boxes of the halos of this warp's particles: the lanes
+// of one halo reduce their ranges, and one of them updates the halo's box.
+// c: stencil cell ranges of the lane's particle; h < 0 for none.
+__device__ __forceinline__ void box_update(int32_t *__restrict__ boxes, int h, bool dep, const int (&c)[6]) {
+    const unsigned grp = __match_any_sync(0xffffffffu, h);
+    if (h < 0) return;
+    int ev[6], dp[6];
+#pragma unroll
+    for (int a = 0; a < 6; a += 2) {
+        ev[a] = __reduce_min_sync(grp, c[a]);
+        ev[a + 1] = __reduce_max_sync(grp, c[a + 1]);
+        dp[a] = __reduce_min_sync(grp, dep ? c[a] : INT_MAX);
+        dp[a + 1] = __reduce_max_sync(grp, dep ? c[a + 1] : INT_MIN);
+    }
+    if ((threadIdx.x & 31) != __ffs(grp) - 1) return;
+    int32_t *b = boxes + (int64_t)kMeshBoxInts * h;
+#pragma unroll
+    for (int a = 0; a < 6; a += 2) {
+        // a plain read first: most warps of a large halo widen nothing
+        if (dp[a] < __ldcg(b + a)) atomicMin(b + a, dp[a]);
+        if (dp[a + 1] > __ldcg(b + a + 1)) atomicMax(b + a + 1, dp[a + 1]);
+        if (ev[a] < __ldcg(b + 6 + a)) atomicMin(b + 6 + a, ev[a]);
+        if (ev[a + 1] > __ldcg(b + 7 + a)) atomicMax(b + 7 + a, ev[a + 1]);
+    }
+}
 
 __global__ void tsc_deposit_kernel(int64_t n, const double *__restrict__ x,
                                    const double *__restrict__ y, const double *__restrict__ z,
@@ -20,36 +55,54 @@ __global__ void tsc_deposit_kernel(int64_t n, const double *__restrict__ x,
                                    const int32_t *__restrict__ hid,
                                    const gf_mesh_desc *__restrict__ mesh,
                                    float *__restrict__ den, float volfold, int *err,
-                                   const int32_t *__restrict__ order) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        // with an order (the octree's permutation) a warp deposits spatial
-        // neighbours, whose stencils share cache lines of the mesh
-        const int64_t p = order ? (int64_t)order[t] : t;
-        const gf_mesh_desc m = mesh[hid ? hid[p] : 0];
-        if (m.ptype != GF_TYPE_ALL && (type ? type[p] : GF_TYPE_DM) != m.ptype) continue;
-        TscStencil s;
-        float xd1, yd1, zd1;
-        tsc_cells(x[p], y[p], z[p], m, s, xd1, yd1, zd1);
-        if (!tsc_in_mesh(s, m)) {
-            atomicOr(err, GF_ERRBIT_RANGE);
-            continue;
-        }
-        tsc_deposit_weights(s, xd1, yd1, zd1, mass[p]);
-        const int64_t mx = 2 * (m.nx / 2 + 1);
-        float *mesh_h = den + m.off;
+                                   const int32_t *__restrict__ order, int32_t *__restrict__ boxes) {
+    // whole warps step together (the box update reduces over the warp)
+    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x; t0 < n; t0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = t0 + threadIdx.x;
+        int hb = -1;  // halo whose box this particle widens
+        bool dep = false;
+        int c[6];
+        if (t < n) {
+            // with an order (the octree's permutation) a warp deposits spatial
+            // neighbours, whose stencils share cache lines of the mesh
+            const int64_t p = order ? (int64_t)order[t] : t;
+            const int h = hid ? hid[p] : 0;
+            const gf_mesh_desc m = mesh[h];
+            dep = m.ptype == GF_TYPE_ALL || (type ? type[p] : GF_TYPE_DM) == m.ptype;
+            // the stencil of every particle when boxes are wanted (findDen
+            // reads there), else of the deposited ones; on-chip meshes none
+            if (m.ptype != kMeshOnChip && (dep || boxes)) {
+                TscStencil s;
+                float xd1, yd1, zd1;
+                tsc_cells(x[p], y[p], z[p], m, s, xd1, yd1, zd1);
+                if (!tsc_in_mesh(s, m)) {
+                    if (dep) atomicOr(err, GF_ERRBIT_RANGE);
+                } else {
+                    hb = h;
+                    c[0] = (int)s.i[0] - 1; c[1] = (int)s.i[0] + 1;
+                    c[2] = (int)s.j[0] - 1; c[3] = (int)s.j[0] + 1;
+                    c[4] = (int)s.k[0] - 1; c[5] = (int)s.k[0] + 1;
+                    if (dep) {
+                        tsc_deposit_weights(s, xd1, yd1, zd1, mass[p]);
+                        const int64_t mx = 2 * (m.nx / 2 + 1);
+                        float *mesh_h = den + m.off;
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
+                        for (int cc = 0; cc < 3; cc++) {
 #pragma unroll
-            for (int b = 0; b < 3; b++) {
+                            for (int b = 0; b < 3; b++) {
 #pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    // volfold is 1 or an exact power of two (see launch_tsc_deposit)
-                    atomicAdd(mesh_h + s.i[a] + mx * (s.j[b] + (int64_t)m.ny * s.k[c]),
-                              tsc_deposit_value(s, a, b, c, volfold));
+                                for (int a = 0; a < 3; a++) {
+                                    // volfold is 1 or an exact power of two (see launch_tsc_deposit)
+                                    atomicAdd(mesh_h + s.i[a] + mx * (s.j[b] + (int64_t)m.ny * s.k[cc]),
+                                              tsc_deposit_value(s, a, b, cc, volfold));
+                                }
+                            }
+                        }
+                    }
                 }
             }
         }
+        if (boxes) box_update(boxes, hb, dep, c);
     }
 }
 
@@ -124,7 +177,12 @@ double tsc_volfact() {
 int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y,
                        const double *z, const double *mass, const int32_t *type,
                        const int32_t *hid, const gf_mesh_desc *mesh, float *den,
-                       double volfact, const int32_t *order) {
+                       double volfact, const int32_t *order, int32_t nhalo, int32_t *boxes) {
+    if (boxes) {
+        const int64_t nint = (int64_t)kMeshBoxInts * std::max(nhalo, 1);
+        box_init_kernel<<<grid_for(nint, 256), 256, 0, ctx->stream>>>(boxes, nint);
+        GF_LAUNCH_CHECK();
+    }
     if (n <= 0) return GF_OK;
     // A power-of-two volfact commutes with every float rounding, so folding
     // it into the weights gives the same bits as the reference's final
@@ -132,7 +190,7 @@ int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y,
     float fold = is_pow2_double(volfact) ? (float)volfact : 1.f;
     const int block = 256;
     tsc_deposit_kernel<<<grid_for(n, block), block, 0, ctx->stream>>>(
-        n, x, y, z, mass, type, hid, mesh, den, fold, ctx->d_err, order);
+        n, x, y, z, mass, type, hid, mesh, den, fold, ctx->d_err, order, boxes);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }

@@ -25,6 +25,9 @@
 #ifndef GF_KNNB_SEEDS  // tree-order neighbours that seed each query's heap (float-key kernel)
 #define GF_KNNB_SEEDS 64
 #endif
+#ifndef GF_KNNB_LANECERT  // float-key kernel: 1 = each lane certifies its own query, 0 = the warp, query by query
+#define GF_KNNB_LANECERT 0
+#endif
 #ifndef GF_KNNB_QUEUE  // float-key kernel: survivors queued per lane (0: inserted at once)
 #define GF_KNNB_QUEUE 0
 #endif
@@ -58,6 +61,7 @@ static_assert(GF_KNN_CHUNK >= 1, "GF_KNN_CHUNK");
 static_assert(GF_KNNB_BLOCK % 32 == 0 && GF_KNNB_BLOCK <= 512, "GF_KNNB_BLOCK");
 static_assert(GF_KNN_ALGO >= 0 && GF_KNN_ALGO <= 2, "GF_KNN_ALGO");
 static_assert(GF_KNNB_ARITY == 2 || GF_KNNB_ARITY == 4, "GF_KNNB_ARITY");
+static_assert(GF_KNNB_LANECERT == 0 || GF_KNNB_LANECERT == 1, "GF_KNNB_LANECERT");
 static_assert(GF_KNNB_QUEUE >= 0 && GF_KNNB_QUEUE <= 16, "GF_KNNB_QUEUE");
 static_assert(GF_KNNB_SEEDS >= 32 && GF_KNNB_SEEDS % 2 == 0, "GF_KNNB_SEEDS");
 static_assert(GF_BH_BLOCK % 32 == 0 && GF_BH_BLOCK <= 1024, "GF_BH_BLOCK");

@@ -11,7 +11,8 @@ result goes to galaxyfinder_b200/tuned.json (parameters, every measurement,
 the GPU and the workload), which build.py turns into -D flags.
 
   group   parameters                                   phase
-  knn     GF_KNN_ALGO x GF_KNNB_BLOCK (x GF_KNNB_ARITY), then GF_KNNB_SEEDS for the
+  knn     GF_KNN_ALGO x GF_KNNB_BLOCK (x GF_KNNB_ARITY), then GF_KNNB_SEEDS,
+          GF_KNNB_LANECERT and GF_KNNB_QUEUE for the
           float-key kernel; for the warp-per-query
           kernel GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
   bh      GF_BH_BLOCK, then the register cap           potential
@@ -36,7 +37,7 @@ from pathlib import Path
 from . import build as B
 
 TUNE_DIR = B.PKG / "_tune"
-DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0,
+DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0, "GF_KNNB_LANECERT": 0,
             "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
             "GF_BH_BLOCK": 128, "GF_BH_ALGO": 0,
             "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TREE_BLOCK": 256}
@@ -52,9 +53,10 @@ def minb(block: int, regs: int) -> int:
 def stages(group: str):
     if group == "knn":
         return [lambda base: [{"GF_KNN_ALGO": a, "GF_KNNB_BLOCK": b, "GF_KNNB_ARITY": 2}
-                              for a in (1, 2) for b in (32, 64)] +
+                              for a in (1, 2) for b in (32, 64, 128)] +
                 [{"GF_KNN_ALGO": 1, "GF_KNNB_BLOCK": 32, "GF_KNNB_ARITY": 4}, {"GF_KNN_ALGO": 0}],
-                lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_SEEDS": n} for n in (32, 48, 64, 96)],
+                lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_SEEDS": n} for n in (32, 48, 64, 80, 96)],
+                lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_LANECERT": c} for c in (0, 1)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_QUEUE": q} for q in (0, 2, 4, 8)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else

@@ -435,6 +435,9 @@ typedef struct gf_stage_stats {
     /* meshes: floats laid out in device memory (mesh_cells counts every
      * planned mesh), and the meshes and particles of the on-chip path */
     int64_t mesh_cells_device, onchip_meshes, onchip_particles;
+    /* cells of the pencils the three smoothing passes filtered, summed over
+     * the passes (3 * mesh_cells_device without the occupied-box skips) */
+    int64_t mesh_pass_cells;
 } gf_stage_stats;
 
 /* stats may be NULL; when given, per-phase CUDA-event times are filled in. */

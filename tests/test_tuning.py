@@ -10,6 +10,7 @@ def _valid(p):
     assert p["GF_KNN_ALGO"] in (0, 1, 2)
     assert p["GF_KNNB_SEEDS"] >= 32 and p["GF_KNNB_SEEDS"] % 2 == 0
     assert 0 <= p["GF_KNNB_QUEUE"] <= 16
+    assert p["GF_KNNB_LANECERT"] in (0, 1)
     assert p["GF_KNNB_BLOCK"] % 32 == 0 and p["GF_KNNB_BLOCK"] <= 512
     assert p["GF_KNN_BLOCK"] % 32 == 0 and p["GF_KNN_BLOCK"] <= 1024
     assert p["GF_BH_BLOCK"] % 32 == 0 and p["GF_BH_BLOCK"] <= 1024
@@ -32,9 +33,10 @@ def test_search_space_is_valid():
                 for ov in stage:
                     _valid(dict(base, **ov))
             assert nonempty >= 1
-        assert len(T.stages("knn")[1](base)) == (4 if algo == 2 else 0)  # seed windows
-        assert len(T.stages("knn")[2](base)) == (4 if algo == 2 else 0)  # survivor queues
-        assert len(T.stages("knn")[3](base)) == (3 if algo == 0 else 0)
+        assert len(T.stages("knn")[1](base)) == (5 if algo == 2 else 0)  # seed windows
+        assert len(T.stages("knn")[2](base)) == (2 if algo == 2 else 0)  # lane or warp certification
+        assert len(T.stages("knn")[3](base)) == (4 if algo == 2 else 0)  # survivor queues
+        assert len(T.stages("knn")[4](base)) == (3 if algo == 0 else 0)
 
 
 def test_tuned_params_become_flags(tmp_path, monkeypatch):
