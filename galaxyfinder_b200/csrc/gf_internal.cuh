@@ -160,6 +160,14 @@ int launch_tsc_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y,
                        const double *mass, const int32_t *type, const int32_t *hid,
                        const gf_mesh_desc *mesh, float *den, double volfact,
                        const int32_t *order = nullptr, int32_t nhalo = 0, int32_t *boxes = nullptr);
+// The stage's deposit (gf_tsc.cu): with GF_TSC_TILE > 0 and an octree
+// order (order = tree order -> batch index, thalo = tree order -> halo; the
+// halos' tree-order ranges are pstart's) through shared-memory tiles, else
+// launch_tsc_deposit in batch order.  Fills the occupied boxes when given.
+int launch_stage_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                         const double *mass, const int32_t *type, const int32_t *hid, const int64_t *pstart,
+                         const int32_t *order, const int32_t *thalo, int32_t nhalo, const gf_mesh_desc *mesh,
+                         float *den, double volfact, int32_t *boxes);
 int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
                     const int32_t *hid, const gf_mesh_desc *mesh, const float *den, float *densph,
                     const int32_t *order = nullptr);

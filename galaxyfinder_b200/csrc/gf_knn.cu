@@ -743,8 +743,12 @@ knn_bucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_
 // distances, and the list is exact when the largest kept exact distance is
 // below min(frej (1 - 2e-6), dbox^2).  A query that fails (near-ties at the
 // k-th place, duplicate positions) goes to a device list that knn_kernel
-// then serves exactly.  Output rows and densities are written by the warp one
-// query at a time (coalesced), in the arithmetic of knn_kernel.
+// then serves exactly.  The certification, the output row and the density
+// (in the arithmetic of knn_kernel) are computed either by every lane for its
+// own query (GF_KNNB_LANECERT=1: the lane heapsorts its column, computes the
+// exact distances in that order and insertion-sorts only where near-ties
+// reversed the float order) or by the warp one query at a time with a
+// bitonic sort of the exact keys.
 constexpr int kFBucketWarpBytes = 32 * 32 * 8 + 32 * (int)sizeof(KnnNode) + 32 * 16 + 32 * 4 +
                                   32 * GF_KNNB_QUEUE * 8;
 

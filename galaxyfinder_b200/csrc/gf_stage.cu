@@ -250,8 +250,9 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         // last pass the columns no particle's findDen stencil reads
         GF_TRY(ctx->mesh_boxes.reserve(sizeof(int32_t) * kMeshBoxInts * (size_t)std::max(nh, 1)));
         int32_t *boxes = ctx->mesh_boxes.as<int32_t>();
-        GF_TRY(launch_tsc_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, mesh_dev, den, vf, nullptr, nh,
-                                  boxes));
+        GF_TRY(launch_stage_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, b->pstart,
+                                    need_tree ? ctx->last_tree.perm : nullptr,
+                                    need_tree ? ctx->last_tree.phalo : nullptr, nh, mesh_dev, den, vf, boxes));
         if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, dev_cells, vf));
         tm.mark();  // 4
         OnChipMeshes oc;

@@ -52,6 +52,9 @@
 #ifndef GF_FFT_PENCILS_128 // real pencils per tile of the 128-cell FFT axes
 #define GF_FFT_PENCILS_128 32
 #endif
+#ifndef GF_TSC_TILE  // cells of the stage deposit's shared-memory tile (0: direct global atomics)
+#define GF_TSC_TILE 0
+#endif
 #ifndef GF_TREE_BLOCK  // threads per block of the per-particle tree-build kernels
 #define GF_TREE_BLOCK 256
 #endif
@@ -71,4 +74,5 @@ static_assert(GF_FFT_PENCILS_64 >= 32 && GF_FFT_PENCILS_64 <= 128 &&
                   (GF_FFT_PENCILS_64 & (GF_FFT_PENCILS_64 - 1)) == 0, "GF_FFT_PENCILS_64");
 static_assert(GF_FFT_PENCILS_128 >= 32 && GF_FFT_PENCILS_128 <= 64 &&
                   (GF_FFT_PENCILS_128 & (GF_FFT_PENCILS_128 - 1)) == 0, "GF_FFT_PENCILS_128");
+static_assert(GF_TSC_TILE == 0 || (GF_TSC_TILE >= 1024 && GF_TSC_TILE <= 12288), "GF_TSC_TILE");
 static_assert(GF_TREE_BLOCK % 32 == 0 && GF_TREE_BLOCK >= 128 && GF_TREE_BLOCK <= 1024, "GF_TREE_BLOCK");

@@ -17,6 +17,7 @@ the GPU and the workload), which build.py turns into -D flags.
           kernel GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
   bh      GF_BH_BLOCK, then the register cap           potential
   fft     GF_FFT_PENCILS                               smooth
+  tsc     GF_TSC_TILE (0: direct global atomics)       tsc
   tree    GF_TREE_BLOCK                                tree
 
 The register cap is expressed as GF_*_MINB = 65536 / (block * registers).
@@ -40,7 +41,7 @@ TUNE_DIR = B.PKG / "_tune"
 DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0, "GF_KNNB_LANECERT": 0,
             "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
             "GF_BH_BLOCK": 128, "GF_BH_ALGO": 0,
-            "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TREE_BLOCK": 256}
+            "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TSC_TILE": 0, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
 
 
@@ -69,13 +70,15 @@ def stages(group: str):
         return [lambda base: [{"GF_FFT_PENCILS": p} for p in (16, 32)],
                 lambda base: [{"GF_FFT_PENCILS_64": p} for p in (32, 64, 128)],
                 lambda base: [{"GF_FFT_PENCILS_128": p} for p in (32, 64)]]
+    if group == "tsc":
+        return [lambda base: [{"GF_TSC_TILE": c} for c in (0, 4096, 8192)]]
     if group == "tree":
         return [lambda base: [{"GF_TREE_BLOCK": b} for b in (128, 256, 512)]]
     raise ValueError(group)
 
 
 GROUPS = {"knn": ("gf_knn.cu", "knn"), "bh": ("gf_potent.cu", "potential"),
-          "fft": ("gf_smooth.cu", "smooth"), "tree": ("gf_tree.cu", "tree")}
+          "fft": ("gf_smooth.cu", "smooth"), "tsc": ("gf_tsc.cu", "tsc"), "tree": ("gf_tree.cu", "tree")}
 
 
 def variant_name(params: dict) -> str:
@@ -127,7 +130,7 @@ def _measure_main(nhalo: int, steps: int) -> None:
     print(json.dumps(best))
 
 
-def tune(nhalo: int, steps: int, groups=("knn", "bh", "fft", "tree")) -> dict:
+def tune(nhalo: int, steps: int, groups=("knn", "bh", "fft", "tsc", "tree")) -> dict:
     B.build()
     base = dict(DEFAULTS)
     base.update(B.tuned_params())
@@ -171,7 +174,7 @@ def main() -> None:
     ap.add_argument("--nhalo", type=int, default=4096)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--measure", action="store_true")
-    ap.add_argument("--groups", default="knn,bh,fft,tree")
+    ap.add_argument("--groups", default="knn,bh,fft,tsc,tree")
     a = ap.parse_args()
     if a.measure:
         _measure_main(a.nhalo, a.steps)

@@ -17,6 +17,7 @@ def _valid(p):
     assert p["GF_FFT_PENCILS"] % 2 == 0 and (p["GF_FFT_PENCILS"] // 2) * 512 // 8 <= 1024
     assert p["GF_FFT_PENCILS_64"] in (32, 64, 128) and p["GF_FFT_PENCILS_128"] in (32, 64)
     assert 128 <= p["GF_TREE_BLOCK"] <= 1024
+    assert p["GF_TSC_TILE"] == 0 or 1024 <= p["GF_TSC_TILE"] <= 12288
     for b, m in ((p["GF_KNN_BLOCK"], p["GF_KNN_MINB"]), (p["GF_BH_BLOCK"], p["GF_BH_MINB"])):
         assert m >= 1 and b * m <= 2048  # resident threads per SM
 
