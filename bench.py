@@ -443,6 +443,52 @@ def postprocessing_workload(dev, steps: int, warmup: int, nchunk: int = 16, bloc
                                                         "p90": float(np.quantile(offs, 0.9)) if len(offs) else None}}}
 
 
+def graph_measurements(args, hb, cfg, ctx, db, out, total_particles, barrier, max_over_ranks) -> dict:
+    """Throughput of CUDA-graph replays of the stage: the whole catalogue as
+    one graph (gf_stage_graph on one stream), and the pipelined stage with
+    one graph per halo chunk; a replay that no longer fits its plan would
+    raise after the timed region."""
+    import torch
+
+    from galaxyfinder_b200 import batch
+    if cfg.mesh_onchip:
+        return {"skipped": "stage graphs capture device-memory meshes only (mesh_onchip is set)"}
+    res = {}
+    g = batch.StageGraph(ctx, db, cfg, out)
+    kernels, nodes = g.nodes()
+    for _ in range(max(args.warmup, 3)):
+        g.launch()
+    g.sync()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ctx.stream)
+    for _ in range(args.steps):
+        g.launch()
+    e1.record(ctx.stream)
+    g.sync()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    res["single_stream"] = {"value": total_particles / (ms / 1e3), "ms_per_step": ms,
+                            "kernel_nodes": kernels, "graph_nodes": nodes, "replans": g.replans,
+                            "path": "gf_stage_graph over the whole catalogue, one replay per step"}
+    g.close()
+    gp = batch.PipelinedStage(hb, cfg, nchunk=args.chunks, device=ctx.device, k=K_NEIGH, graph=True)
+    for mode in ("resident", "e2e"):
+        runner = gp.run_resident if mode == "resident" else gp.run_e2e
+        runner(max(args.warmup, 3))
+        gp.check()
+        barrier()
+        p0, p1 = runner(args.steps)
+        torch.cuda.synchronize()
+        gp.check()
+        pms = max_over_ranks(p0.elapsed_time(p1) / args.steps)
+        res["pipelined_" + mode] = {"value": total_particles / (pms / 1e3), "ms_per_step": pms}
+    res["pipelined_resident"]["path"] = (f"PipelinedStage(graph=True): {len(gp.chunks)} halo chunks, each "
+                                         "replaying its own captured stage")
+    gp.close()
+    torch.cuda.synchronize()
+    return res
+
+
 def workload_config(args, hb, world: int, mesh_cells: int) -> dict:
     """The `config` object of both arms' JSON lines."""
     return {"workload": f"batched catalogue, {args.nhalo} FoF halos per GPU, N_p ~ N^-1.9 on [100, 2e6], "
@@ -730,11 +776,16 @@ def main():
         pms = max_over_ranks(p0.elapsed_time(p1) / args.steps)
         pipe_res[mode] = {"value": total_particles / (pms / 1e3), "ms_per_step": pms,
                           "launches": (lib.gf_kernel_launch_count() - l0) // max(args.steps, 1)}
-    clk = clocks.stop()
     nchunks = len(pipe.chunks)
     pipe_h2d, pipe_d2h = int(pipe.h2d_bytes), int(pipe.d2h_bytes)
     pipe.close()
     del pipe
+
+    # ---- the stage captured as CUDA graphs: the whole catalogue as one graph
+    # on one stream, and each chunk of the pipelined stage as its own graph;
+    # every replay runs every kernel of the stage on the resident inputs
+    graph_res = graph_measurements(args, hb, cfg, ctx, db, out, total_particles, barrier, max_over_ranks)
+    clk = clocks.stop()
 
     # ---- plain GPU path: every phase in FP64 (plain_fp64), one halo per
     # gf_stage_run call, inputs resident; and, for the batching's own gain,
@@ -864,6 +915,7 @@ def main():
         "knn_work_per_query": knn_work,
         "plain": plain,
         "gpu_launches": int(pipe_res["resident"]["launches"]),
+        "graph": graph_res,
         "clocks": clk,
     })
 

@@ -16,7 +16,7 @@ import numpy as np
 LIB_PATH = Path(os.environ.get("GF_LIBGF") or Path(__file__).resolve().parent / "libgf.so")
 
 # status codes (gf.h)
-GF_OK, GF_EINVAL, GF_ENOMEM, GF_EDEVICE, GF_ETIMEOUT, GF_ERANGE, GF_ENOTIMPL = range(7)
+GF_OK, GF_EINVAL, GF_ENOMEM, GF_EDEVICE, GF_ETIMEOUT, GF_ERANGE, GF_ENOTIMPL, GF_ESTALE = range(8)
 
 # particle types (NewGalFinder/tree.h:47-48)
 TYPE_STAR, TYPE_DM, TYPE_GAS, TYPE_SINK, TYPE_ALL = 1, 2, 3, 4, 5
@@ -224,6 +224,14 @@ SIGNATURES = {
     "gf_bg_potent_device": (_INT, [_VP, _I32, _VP, _VP]),
     "gf_stage_run": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),
                             ctypes.POINTER(StageOut), ctypes.POINTER(StageStats)]),
+    "gf_stage_graph_create": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),
+                                     ctypes.POINTER(StageOut), ctypes.POINTER(_VP)]),
+    "gf_stage_graph_launch": (_INT, [_VP]),
+    "gf_stage_graph_sync": (_INT, [_VP]),
+    "gf_stage_graph_run": (_INT, [_VP, ctypes.POINTER(_I32)]),
+    "gf_stage_graph_replans": (_INT, [_VP]),
+    "gf_stage_graph_nodes": (_INT, [_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    "gf_stage_graph_destroy": (None, [_VP]),
 }
 
 

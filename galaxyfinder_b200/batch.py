@@ -223,6 +223,59 @@ def stage_run(ctx: Context, batch: DeviceBatch, cfg: _lib.StageConfig,
     return out
 
 
+class StageGraph:
+    """The stage of one batch captured as a CUDA graph (gf_stage_graph_*).
+
+    Creating it runs the stage once eagerly (its outputs are the batch's
+    results) and captures a pass with every launch shape fixed by that run's
+    plan.  launch() replays it on the batch's current contents, asynchronously
+    on the context's stream; sync() waits and raises GFError(GF_ESTALE) if a
+    replay no longer fitted the plan.  run() replays, waits and re-plans when
+    needed (returns True then).  The batch and output tensors must stay alive
+    and in place while the graph exists."""
+
+    def __init__(self, ctx: Context, batch: DeviceBatch, cfg: _lib.StageConfig, out: StageBuffers):
+        self.ctx, self.batch, self.cfg, self.out = ctx, batch, cfg, out
+        self._b = batch.c()
+        self._o = out.c()
+        h = ctypes.c_void_p()
+        check(lib().gf_stage_graph_create(ctx.handle, ctypes.byref(self._b), ctypes.byref(cfg),
+                                          ctypes.byref(self._o), ctypes.byref(h)))
+        self.handle = h
+
+    def launch(self):
+        check(lib().gf_stage_graph_launch(self.handle))
+
+    def sync(self):
+        check(lib().gf_stage_graph_sync(self.handle))
+
+    def run(self) -> bool:
+        replanned = ctypes.c_int32()
+        check(lib().gf_stage_graph_run(self.handle, ctypes.byref(replanned)))
+        return bool(replanned.value)
+
+    @property
+    def replans(self) -> int:
+        return int(lib().gf_stage_graph_replans(self.handle))
+
+    def nodes(self):
+        """(kernel nodes, all nodes) of the captured graph."""
+        k, n = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().gf_stage_graph_nodes(self.handle, ctypes.byref(k), ctypes.byref(n)))
+        return k.value, n.value
+
+    def close(self):
+        if self.handle:
+            lib().gf_stage_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def density_peaks(ctx: Context, den, neighbor, type_=None, threshold=2000.0):
     """finddenpeak's peaks (subhaloden.mod6.c:416-494) of one halo on the
     device: den (np,) float32, neighbor (np, k) int32 halo-local kNN lists,
@@ -285,7 +338,7 @@ class PipelinedStage:
     chunks' passes."""
 
     def __init__(self, hb, cfg: _lib.StageConfig, nchunk: int = 3, device: int = 0, k: int = 32,
-                 prioritise: bool = True):
+                 prioritise: bool = True, graph: bool = False):
         import concurrent.futures as cf
         self.cfg = cfg
         self.k = k
@@ -314,6 +367,11 @@ class PipelinedStage:
                     for f in ("nearindex", "dens_sph", "dens_mesh", "penergy")}
             self.chunks.append(dict(ctx=ctx, stream=stream, host=host, db=db, out=out, hout=hout, n=p1 - p0))
         torch.cuda.synchronize(dev)
+        # with `graph`, each chunk's stage is captured once and replayed
+        self.graph = graph
+        for c in self.chunks:
+            c["graph"] = StageGraph(c["ctx"], c["db"], cfg, c["out"]) if graph else None
+        torch.cuda.synchronize(dev)
         self.pool = cf.ThreadPoolExecutor(max_workers=len(self.chunks))
         self.h2d_bytes = sum(t.numel() * t.element_size() for c in self.chunks for t in c["host"].values())
         self.d2h_bytes = sum(t.numel() * t.element_size() for c in self.chunks for t in c["hout"].values())
@@ -326,7 +384,10 @@ class PipelinedStage:
                 with torch.cuda.stream(s):
                     for f in ("x", "y", "z", "mass", "type", "pstart"):
                         getattr(c["db"], f).copy_(c["host"][f], non_blocking=True)
-            stage_run(c["ctx"], c["db"], self.cfg, c["out"])
+            if c["graph"] is not None:
+                c["graph"].launch()
+            else:
+                stage_run(c["ctx"], c["db"], self.cfg, c["out"])
             if e2e:
                 with torch.cuda.stream(s):
                     for f, t in c["hout"].items():
@@ -353,7 +414,16 @@ class PipelinedStage:
     def run_e2e(self, steps: int = 1):
         return self._run(True, steps)
 
+    def check(self):
+        """With graphs: waits for every chunk and raises GFError(GF_ESTALE) if
+        a replay no longer fitted its chunk's plan."""
+        for c in self.chunks:
+            if c["graph"] is not None:
+                c["graph"].sync()
+
     def close(self):
         self.pool.shutdown()
         for c in self.chunks:
+            if c.get("graph") is not None:
+                c["graph"].close()
             c["ctx"].close()

@@ -146,6 +146,10 @@ int check_device_errors(gf_ctx *ctx) {
     GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (h) {
         GF_CUDA_TRY(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        if (h & GF_ERRBIT_PLAN) {
+            set_status(GF_ESTALE, "the batch no longer fits the captured stage plan");
+            return GF_ESTALE;
+        }
         if (h & GF_ERRBIT_RANGE) {
             set_status(GF_ERANGE, "a particle's TSC stencil falls outside its mesh");
             return GF_ERANGE;
@@ -294,6 +298,7 @@ const char *gf_status_string(int status) {
         case GF_ETIMEOUT: return "device wait timed out";
         case GF_ERANGE: return "particle outside mesh";
         case GF_ENOTIMPL: return "not implemented";
+        case GF_ESTALE: return "stage graph plan no longer fits the batch";
         default: return "unknown status";
     }
 }
@@ -323,7 +328,10 @@ int gf_tuning_value(const char *name, int64_t *value) {
                   {"GF_KNN_BLOCK", GF_KNN_BLOCK},
                   {"GF_KNN_MINB", GF_KNN_MINB},       {"GF_KNN_CHUNK", GF_KNN_CHUNK},
                   {"GF_BH_BLOCK", GF_BH_BLOCK},       {"GF_BH_MINB", GF_BH_MINB},
-                  {"GF_FFT_PENCILS", GF_FFT_PENCILS}, {"GF_TREE_BLOCK", GF_TREE_BLOCK}};
+                  {"GF_FFT_PENCILS", GF_FFT_PENCILS}, {"GF_TREE_BLOCK", GF_TREE_BLOCK},
+                  {"GF_KNNB_QUEUE", GF_KNNB_QUEUE},   {"GF_KNNB_LANECERT", GF_KNNB_LANECERT},
+                  {"GF_BH_ALGO", GF_BH_ALGO},         {"GF_FFT_PENCILS_64", GF_FFT_PENCILS_64},
+                  {"GF_FFT_PENCILS_128", GF_FFT_PENCILS_128}, {"GF_TSC_TILE", GF_TSC_TILE}};
     if (!name || !value) return GF_EINVAL;
     for (const auto &p : params)
         if (strcmp(p.name, name) == 0) {

@@ -62,6 +62,7 @@ enum : int {
     GF_ERRBIT_KNN = 4,        // a kNN query found fewer than k neighbours
     GF_ERRBIT_WALK = 8,       // a tree walk exceeded its step bound
     GF_ERRBIT_INDEX = 16,     // an index argument (query, neighbour) is out of range
+    GF_ERRBIT_PLAN = 32,      // the batch no longer fits a captured stage plan
 };
 
 // ---------------------------------------------------------------- workspace
@@ -195,6 +196,24 @@ struct MeshBoxes {
 int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
                   const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip = nullptr,
                   const MeshBoxes *boxes = nullptr);
+// smooth_meshes in two steps: the host plan (axis tables, per-(axis, length)
+// tile groups) in one blob, and the launches once the blob is in device
+// memory at dbuf (a CUDA graph uploads it once and captures the launches).
+struct SmoothGroup {
+    int axis, n, pmax;
+    size_t off_halos, off_starts;  // blob offsets: halo list, tile prefix
+    int32_t ngroup;
+    int64_t ntiles;
+};
+struct SmoothPlan {
+    std::vector<char> blob;  // [axes | tables | on-chip halos | per group: halos, starts]
+    size_t off_tab = 0, off_chip = 0;
+    int32_t nchip = 0;
+    std::vector<SmoothGroup> groups;
+};
+int smooth_plan(int32_t nhalo, const gf_mesh_desc *mesh_host, const OnChipMeshes *onchip, SmoothPlan *plan);
+int smooth_launch(gf_ctx *ctx, const SmoothPlan &plan, const char *dbuf, const gf_mesh_desc *mesh_dev,
+                  float *den, const OnChipMeshes *onchip = nullptr, const MeshBoxes *boxes = nullptr);
 
 // Single-mesh smoothing plan in one contiguous byte blob (see gf_smooth.cu):
 // [mesh desc | 3 axis tables | per axis: halo list, tile prefix | tables].
@@ -220,7 +239,16 @@ int halo_frames(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, double box,
 // FP64 recentring (Dump2BP) -> double SoA + float4 (x, y, z, mass).
 int recentre(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, const double *frame_dev,
              double box, double *xr, double *yr, double *zr, float4 *pos);
-gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r);
+__host__ __device__ gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r);
+// Graph mode: frames and meshes computed on the device from the extents that
+// the same pass found (ext: the extent kernel's keys, as halo_frames reads
+// them).  Each mesh must keep the shape of `planned` (nx, ny, nz, the float
+// rg/cellsize its smoothing tables were built for); otherwise the kernel sets
+// GF_ERRBIT_PLAN.  Offsets and ptype come from `planned`.
+int launch_frames_plan(gf_ctx *ctx, int32_t nhalo, double box, const gf_mesh_rule &rule, int do_mesh,
+                       const gf_mesh_desc *planned, double *frame_dev, gf_mesh_desc *mesh_dev);
+// The extent kernels alone (keys into ctx->tmp[6]), for graph mode.
+int launch_extents(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, double box);
 
 // volfact of tsc_omp2.c:188 for the reference cell size 0.004 cMpc/h.
 double tsc_volfact();

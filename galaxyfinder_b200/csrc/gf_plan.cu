@@ -113,6 +113,17 @@ int grid1d(int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(g, sm_count() * 16));
 }
 
+// Frame and extent of one axis from the extent keys (halo_frames' rule).
+__host__ __device__ inline void axis_frame(const unsigned long long *k, double box, double &origin,
+                                           double &shift, double &extent) {
+    const double lo = dkey_inv(k[0]), hi = dkey_inv(k[1]);
+    const double los = dkey_inv(k[2]), his = dkey_inv(k[3]);
+    const bool sh = box > 0 && (hi - lo) > 0.5 * box && (his - los) < (hi - lo);
+    origin = sh ? los : lo;
+    shift = sh ? 1.0 : 0.0;
+    extent = sh ? his - los : hi - lo;
+}
+
 }  // namespace
 
 int halo_frames(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, double box,
@@ -130,17 +141,10 @@ int halo_frames(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, double box,
     GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     frame_host.assign(6 * (size_t)nh, 0.0);
     extent_host.assign(3 * (size_t)nh, 0.0);
-    for (int h = 0; h < nh; h++) {
-        for (int a = 0; a < 3; a++) {
-            const unsigned long long *k = &hk[12 * (size_t)h + 4 * a];
-            double lo = dkey_inv(k[0]), hi = dkey_inv(k[1]);
-            double los = dkey_inv(k[2]), his = dkey_inv(k[3]);
-            bool shift = box > 0 && (hi - lo) > 0.5 * box && (his - los) < (hi - lo);
-            frame_host[6 * (size_t)h + 2 * a] = shift ? los : lo;
-            frame_host[6 * (size_t)h + 2 * a + 1] = shift ? 1.0 : 0.0;
-            extent_host[3 * (size_t)h + a] = shift ? his - los : hi - lo;
-        }
-    }
+    for (int h = 0; h < nh; h++)
+        for (int a = 0; a < 3; a++)
+            axis_frame(&hk[12 * (size_t)h + 4 * a], box, frame_host[6 * (size_t)h + 2 * a],
+                       frame_host[6 * (size_t)h + 2 * a + 1], extent_host[3 * (size_t)h + a]);
     return GF_OK;
 }
 
@@ -153,8 +157,10 @@ int recentre(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, const double *f
     return GF_OK;
 }
 
-// Mesh of one halo from its recentred extent (min = 0 on every axis).
-gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r) {
+// Mesh of one halo from its recentred extent (min = 0 on every axis).  Host
+// and device run the same double arithmetic (this file is compiled with
+// --fmad=false), so a mesh planned on the device equals the host's plan.
+__host__ __device__ gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r) {
     gf_mesh_desc m{};
     m.ptype = r.ptype;
     const int nb = r.nbuff;
@@ -167,7 +173,7 @@ gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r) {
         // nnost.c:1053-1055: n = extent/cellsize + nbuff per axis
         for (int a = 0; a < 3; a++) n[a] = (int)(e[a] / cs + nb);
     } else {
-        const double w = std::max(e[0], std::max(e[1], e[2]));
+        const double w = e[0] > (e[1] > e[2] ? e[1] : e[2]) ? e[0] : (e[1] > e[2] ? e[1] : e[2]);
         int nc;
         if (r.mode == GF_MESH_FIXED) {
             nc = r.nfixed;
@@ -177,8 +183,10 @@ gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r) {
             const double need = w / r.cell + nb;
             nc = 1;
             while (nc < need && nc < (1 << 20)) nc <<= 1;
-            nc = std::min(std::max(nc, r.nmin), r.nmax);
-            cs = std::max(r.cell, w / (double)(nc - nb));
+            nc = nc > r.nmin ? nc : r.nmin;
+            nc = nc < r.nmax ? nc : r.nmax;
+            const double c2 = w / (double)(nc - nb);
+            cs = r.cell > c2 ? r.cell : c2;
         }
         n[0] = n[1] = n[2] = nc;
     }
@@ -192,6 +200,59 @@ gf_mesh_desc plan_one_mesh(const double ext[3], const gf_mesh_rule &r) {
     m.zmin = 0.0 - cs * nb / 2.;
     m.rg = r.rg_in_cells ? r.rg * cs : r.rg;
     return m;
+}
+
+namespace {
+
+__global__ void frames_plan_kernel(int32_t nhalo, const unsigned long long *__restrict__ ext, double box,
+                                   gf_mesh_rule rule, int do_mesh, const gf_mesh_desc *__restrict__ planned,
+                                   double *__restrict__ frame, gf_mesh_desc *__restrict__ mesh, int *err) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= nhalo) return;
+    double e[3];
+    for (int a = 0; a < 3; a++)
+        axis_frame(ext + 12 * (int64_t)h + 4 * a, box, frame[6 * (int64_t)h + 2 * a],
+                   frame[6 * (int64_t)h + 2 * a + 1], e[a]);
+    if (!do_mesh) return;
+    gf_mesh_desc m = plan_one_mesh(e, rule);
+    const gf_mesh_desc &p = planned[h];
+    // the smoothing tables are keyed by the float rg/cellsize (gsmooth.c:67)
+    if (m.nx != p.nx || m.ny != p.ny || m.nz != p.nz ||
+        (float)(m.rg / m.cellsize) != (float)(p.rg / p.cellsize)) {
+        // the captured mesh stays (its shape bounds every access to its
+        // cells; particles outside it are flagged by the deposit)
+        atomicOr(err, GF_ERRBIT_PLAN);
+        mesh[h] = p;
+        return;
+    }
+    m.off = p.off;
+    m.ptype = p.ptype;
+    mesh[h] = m;
+}
+
+}  // namespace
+
+int launch_extents(gf_ctx *ctx, const gf_batch *b, const int32_t *hid, double box) {
+    const int nh = b->nhalo;
+    GF_TRY(ctx->tmp[6].reserve(sizeof(unsigned long long) * 12 * (size_t)std::max(nh, 1)));
+    unsigned long long *ext = ctx->tmp[6].as<unsigned long long>();
+    extent_init_kernel<<<grid1d(12 * (int64_t)nh), 256, 0, ctx->stream>>>(ext, 12 * (int64_t)nh);
+    GF_LAUNCH_CHECK();
+    if (b->nparticle > 0) {
+        extent_kernel<<<grid1d(b->nparticle), 256, 0, ctx->stream>>>(b->nparticle, b->x, b->y, b->z, hid, box,
+                                                                      ext);
+        GF_LAUNCH_CHECK();
+    }
+    return GF_OK;
+}
+
+int launch_frames_plan(gf_ctx *ctx, int32_t nhalo, double box, const gf_mesh_rule &rule, int do_mesh,
+                       const gf_mesh_desc *planned, double *frame_dev, gf_mesh_desc *mesh_dev) {
+    if (nhalo <= 0) return GF_OK;
+    frames_plan_kernel<<<(nhalo + 127) / 128, 128, 0, ctx->stream>>>(
+        nhalo, ctx->tmp[6].as<unsigned long long>(), box, rule, do_mesh, planned, frame_dev, mesh_dev, ctx->d_err);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
 }
 
 }  // namespace gf

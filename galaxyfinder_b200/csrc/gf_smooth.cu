@@ -783,11 +783,8 @@ int launch_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLau
 
 }  // namespace
 
-int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
-                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip,
-                  const MeshBoxes *boxes) {
-    const int32_t *bx = boxes ? boxes->dev : nullptr;
-    const int trim = boxes && boxes->trim_last ? 1 : 0;
+int smooth_plan(int32_t nhalo, const gf_mesh_desc *mesh_host, const OnChipMeshes *onchip, SmoothPlan *plan) {
+    *plan = SmoothPlan();
     if (nhalo <= 0) return GF_OK;
     const int32_t non_chip = onchip ? onchip->nmesh : 0;  // meshes on chip
     std::vector<AxisTable> axes(3 * (size_t)nhalo);
@@ -859,12 +856,13 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
             g.start.push_back(g.start.back() + c);
         }
     }
-    // one staging buffer: [axes | tables | on-chip halos | per group: halos, starts]
+    // one blob: [axes | tables | on-chip halos | per group: halos, starts]
     auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
     size_t off = align(axes.size() * sizeof(AxisTable));
-    const size_t off_tab = off;
+    plan->off_tab = off;
     off = align(off + tables.size() * sizeof(float));
-    const size_t off_chip = off;
+    plan->off_chip = off;
+    plan->nchip = non_chip;
     off = align(off + (size_t)non_chip * sizeof(int32_t));
     std::vector<size_t> off_h(groups.size()), off_s(groups.size());
     for (size_t i = 0; i < groups.size(); i++) {
@@ -873,38 +871,47 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
         off_s[i] = off;
         off = align(off + groups[i].start.size() * sizeof(int64_t));
     }
-    const size_t total = off;
-    GF_TRY(ctx->smooth_tables.reserve(total));
-    GF_TRY(ctx->pin[3].reserve(total));
-    char *hbuf = ctx->pin[3].as<char>();
-    // the pinned staging buffer may still feed an earlier asynchronous copy
-    GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    plan->blob.assign(off, 0);
+    char *hbuf = plan->blob.data();
     memcpy(hbuf, axes.data(), axes.size() * sizeof(AxisTable));
-    memcpy(hbuf + off_tab, tables.data(), tables.size() * sizeof(float));
-    if (non_chip) memcpy(hbuf + off_chip, onchip->halos_host, (size_t)non_chip * sizeof(int32_t));
+    memcpy(hbuf + plan->off_tab, tables.data(), tables.size() * sizeof(float));
+    if (non_chip) memcpy(hbuf + plan->off_chip, onchip->halos_host, (size_t)non_chip * sizeof(int32_t));
     for (size_t i = 0; i < groups.size(); i++) {
         memcpy(hbuf + off_h[i], groups[i].halos.data(), groups[i].halos.size() * sizeof(int32_t));
         memcpy(hbuf + off_s[i], groups[i].start.data(), groups[i].start.size() * sizeof(int64_t));
+        SmoothGroup sg;
+        sg.axis = groups[i].axis;
+        sg.n = groups[i].n;
+        sg.pmax = groups[i].pmax;
+        sg.off_halos = off_h[i];
+        sg.off_starts = off_s[i];
+        sg.ngroup = (int32_t)groups[i].halos.size();
+        sg.ntiles = groups[i].start.back();
+        plan->groups.push_back(sg);
     }
-    char *dbuf = ctx->smooth_tables.as<char>();
-    GF_CUDA_TRY(cudaMemcpyAsync(dbuf, hbuf, total, cudaMemcpyHostToDevice, ctx->stream));
+    return GF_OK;
+}
+
+int smooth_launch(gf_ctx *ctx, const SmoothPlan &plan, const char *dbuf, const gf_mesh_desc *mesh_dev,
+                  float *den, const OnChipMeshes *onchip, const MeshBoxes *boxes) {
+    if (plan.blob.empty()) return GF_OK;
+    const int32_t *bx = boxes ? boxes->dev : nullptr;
+    const int trim = boxes && boxes->trim_last ? 1 : 0;
     const AxisTable *d_axes = reinterpret_cast<const AxisTable *>(dbuf);
-    const float *d_tab = reinterpret_cast<const float *>(dbuf + off_tab);
-    for (size_t i = 0; i < groups.size(); i++) {
-        const Group &g = groups[i];
+    const float *d_tab = reinterpret_cast<const float *>(dbuf + plan.off_tab);
+    for (const SmoothGroup &g : plan.groups) {
         GroupLaunch gl;
-        gl.halos = reinterpret_cast<const int32_t *>(dbuf + off_h[i]);
-        gl.tile_start = reinterpret_cast<const int64_t *>(dbuf + off_s[i]);
-        gl.ngroup = (int32_t)g.halos.size();
-        const int64_t nt = g.start.back();
-        if (g.axis == 0) GF_TRY(launch_group<0>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab, bx, trim));
-        else if (g.axis == 1) GF_TRY(launch_group<1>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab, bx, trim));
-        else GF_TRY(launch_group<2>(ctx, den, mesh_dev, gl, nt, g.n, g.pmax, d_axes, d_tab, bx, trim));
+        gl.halos = reinterpret_cast<const int32_t *>(dbuf + g.off_halos);
+        gl.tile_start = reinterpret_cast<const int64_t *>(dbuf + g.off_starts);
+        gl.ngroup = g.ngroup;
+        if (g.axis == 0) GF_TRY(launch_group<0>(ctx, den, mesh_dev, gl, g.ntiles, g.n, g.pmax, d_axes, d_tab, bx, trim));
+        else if (g.axis == 1) GF_TRY(launch_group<1>(ctx, den, mesh_dev, gl, g.ntiles, g.n, g.pmax, d_axes, d_tab, bx, trim));
+        else GF_TRY(launch_group<2>(ctx, den, mesh_dev, gl, g.ntiles, g.n, g.pmax, d_axes, d_tab, bx, trim));
     }
-    if (non_chip) {
+    if (plan.nchip) {
         OnChipArgs a;
-        a.nmesh = non_chip;
-        a.halos = reinterpret_cast<const int32_t *>(dbuf + off_chip);
+        a.nmesh = plan.nchip;
+        a.halos = reinterpret_cast<const int32_t *>(dbuf + plan.off_chip);
         a.ptype = onchip->ptype;
         a.pstart = onchip->pstart;
         a.x = onchip->x;
@@ -921,6 +928,23 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
         GF_TRY(launch_onchip(ctx, a));
     }
     return GF_OK;
+}
+
+int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
+                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip,
+                  const MeshBoxes *boxes) {
+    SmoothPlan plan;
+    GF_TRY(smooth_plan(nhalo, mesh_host, onchip, &plan));
+    if (plan.blob.empty()) return GF_OK;
+    const size_t total = plan.blob.size();
+    GF_TRY(ctx->smooth_tables.reserve(total));
+    GF_TRY(ctx->pin[3].reserve(total));
+    // the pinned staging buffer may still feed an earlier asynchronous copy
+    GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    memcpy(ctx->pin[3].ptr, plan.blob.data(), total);
+    char *dbuf = ctx->smooth_tables.as<char>();
+    GF_CUDA_TRY(cudaMemcpyAsync(dbuf, ctx->pin[3].ptr, total, cudaMemcpyHostToDevice, ctx->stream));
+    return smooth_launch(ctx, plan, dbuf, mesh_dev, den, onchip, boxes);
 }
 
 }  // namespace gf

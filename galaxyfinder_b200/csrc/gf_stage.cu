@@ -132,13 +132,14 @@ int gf_self_potential(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *psta
     return check_device_errors(ctx);
 }
 
-// ------------------------------------------------------------------ full stage
-int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *o,
-                 gf_stage_stats *st) {
-    clear_status();
-    if (!ctx || !b || !cfg || !o || b->nhalo < 0 || b->nparticle < 0) return GF_EINVAL;
-    if (b->nparticle > 0 && (!b->pstart || !b->x || !b->y || !b->z || !b->mass)) return GF_EINVAL;
-    std::lock_guard<std::mutex> g(ctx->lock);
+}  // extern "C"
+
+namespace gf {
+
+// The stage on ctx (its lock held); `plan`, when given, receives what a
+// captured pass needs: the meshes, their cell counts and the octree's shape.
+int stage_run_locked(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *o,
+                     gf_stage_stats *st, StagePlan *plan) {
     const int64_t n = b->nparticle;
     const int32_t nh = b->nhalo;
     cudaStream_t s = ctx->stream;
@@ -197,7 +198,15 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
     // ---- 2. octree
     const bool need_tree = cfg->knn_k > 0 || cfg->do_potential;
     if (need_tree)
-        GF_TRY(build_tree(ctx, nh, n, b->pstart, pos, cfg->theta2, cfg->q5_asbuilt, &ctx->last_tree));
+        GF_TRY(build_tree(ctx, nh, n, b->pstart, pos, cfg->theta2, cfg->q5_asbuilt, &ctx->last_tree, nullptr,
+                          plan ? &plan->tree : nullptr));
+    if (plan) {
+        plan->need_tree = need_tree;
+        plan->mesh = mesh;
+        plan->cells = cells;
+        plan->dev_cells = dev_cells;
+        plan->onchip = !onchip_halos.empty();
+    }
     tm.mark();  // 2
     if (cfg->plain_fp64) {
         const double pf = cfg->potentfact != 0.0 ? cfg->potentfact : physics().potentfact;
@@ -354,6 +363,268 @@ int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_
         }
     }
     return status;
+}
+
+}  // namespace gf
+
+extern "C" {
+
+int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *o,
+                 gf_stage_stats *st) {
+    clear_status();
+    if (!ctx || !b || !cfg || !o || b->nhalo < 0 || b->nparticle < 0) return GF_EINVAL;
+    if (b->nparticle > 0 && (!b->pstart || !b->x || !b->y || !b->z || !b->mass)) return GF_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    return stage_run_locked(ctx, b, cfg, o, st, nullptr);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ stage graph
+// The stage captured as one CUDA graph.  An eager run plans it (meshes from
+// the halo extents, the octree's depth and node count); the captured pass
+// then computes the frames and meshes on the device from the same extents,
+// builds the octree with a fixed depth (two levels more than planned) and
+// node capacity (a quarter more) and replays every kernel of the stage with
+// no host round trip.  A replay is valid for any contents of the batch's
+// input buffers whose meshes keep the planned shapes and whose octree fits
+// the fixed shape; otherwise the pass flags GF_ERRBIT_PLAN and the replay
+// reports GF_ESTALE (gf_stage_graph_run then re-plans and re-captures).
+namespace gf {
+
+struct StageGraph {
+    gf_ctx *ctx = nullptr;
+    gf_batch b{};
+    gf_stage_config cfg{};
+    gf_stage_out o{};
+    StagePlan plan;
+    TreeShape fixed;
+    SmoothPlan smooth;
+    DevBuf planned;       // the planned mesh descriptors (device)
+    DevBuf smooth_blob;   // the smoothing plan (device)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<void *> bufs;  // context buffers the graph reads and writes
+    int32_t replans = 0;
+};
+
+namespace {
+
+std::vector<void *> context_buffers(gf_ctx *c) {
+    std::vector<void *> v = {c->hid.ptr, c->mesh.ptr, c->mesh_boxes.ptr, c->smooth_tables.ptr, c->particles.ptr};
+    for (auto &t : c->tmp) v.push_back(t.ptr);
+    for (auto &t : c->tree) v.push_back(t.ptr);
+    return v;
+}
+
+// The stage with every launch shape from the graph's plan: capturable.
+int stage_pass_graph(StageGraph &g) {
+    gf_ctx *ctx = g.ctx;
+    const gf_batch *b = &g.b;
+    const gf_stage_config *cfg = &g.cfg;
+    gf_stage_out *o = &g.o;
+    const int64_t n = b->nparticle;
+    const int32_t nh = b->nhalo;
+    cudaStream_t s = ctx->stream;
+    GF_TRY(ctx->hid.reserve(sizeof(int32_t) * std::max<int64_t>(n, 1)));
+    int32_t *hid = ctx->hid.as<int32_t>();
+    GF_TRY(compute_hid(ctx, nh, n, b->pstart, hid));
+    GF_TRY(launch_extents(ctx, b, hid, cfg->box));
+    const size_t nn = (size_t)std::max<int64_t>(n, 1);
+    const size_t dbytes = (nn * sizeof(double) + 255) & ~size_t(255);
+    GF_TRY(ctx->tmp[2].reserve(3 * dbytes + nn * sizeof(float4) + 256));
+    char *t2 = ctx->tmp[2].as<char>();
+    double *xr = o->xr ? o->xr : reinterpret_cast<double *>(t2);
+    double *yr = o->yr ? o->yr : reinterpret_cast<double *>(t2 + dbytes);
+    double *zr = o->zr ? o->zr : reinterpret_cast<double *>(t2 + 2 * dbytes);
+    float4 *pos = reinterpret_cast<float4 *>(t2 + 3 * dbytes);
+    const size_t frame_bytes = (6 * (size_t)std::max(nh, 1) * sizeof(double) + 255) & ~size_t(255);
+    GF_TRY(ctx->mesh.reserve(frame_bytes + (size_t)std::max(nh, 1) * sizeof(gf_mesh_desc) + 512));
+    double *frame_dev = ctx->mesh.as<double>();
+    gf_mesh_desc *mesh_dev = reinterpret_cast<gf_mesh_desc *>(ctx->mesh.as<char>() + frame_bytes);
+    GF_TRY(launch_frames_plan(ctx, nh, cfg->box, cfg->mesh, cfg->do_mesh, g.planned.as<gf_mesh_desc>(), frame_dev,
+                              mesh_dev));
+    GF_TRY(recentre(ctx, b, hid, frame_dev, cfg->box, xr, yr, zr, pos));
+    if (g.plan.need_tree)
+        GF_TRY(build_tree(ctx, nh, n, b->pstart, pos, cfg->theta2, cfg->q5_asbuilt, &ctx->last_tree, &g.fixed));
+    if (cfg->knn_k > 0)
+        GF_TRY(launch_knn(ctx, ctx->last_tree, b->pstart, pos, cfg->knn_k, o->nearindex, o->dens_sph, nullptr));
+    if (cfg->do_mesh) {
+        const int64_t dev_cells = g.plan.dev_cells;
+        GF_TRY(ctx->tmp[3].reserve(sizeof(float) * (size_t)std::max<int64_t>(dev_cells, 1)));
+        float *den = ctx->tmp[3].as<float>();
+        GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * dev_cells, s));
+        const double vf = tsc_volfact();
+        GF_TRY(ctx->mesh_boxes.reserve(sizeof(int32_t) * kMeshBoxInts * (size_t)std::max(nh, 1)));
+        int32_t *boxes = ctx->mesh_boxes.as<int32_t>();
+        GF_TRY(launch_stage_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, b->pstart,
+                                    g.plan.need_tree ? ctx->last_tree.perm : nullptr,
+                                    g.plan.need_tree ? ctx->last_tree.phalo : nullptr, nh, mesh_dev, den, vf, boxes));
+        if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, dev_cells, vf));
+        MeshBoxes mb;
+        mb.dev = boxes;
+        mb.trim_last = true;  // den is read only by find_den below
+        GF_TRY(smooth_launch(ctx, g.smooth, g.smooth_blob.as<char>(), mesh_dev, den, nullptr, &mb));
+        if (o->dens_mesh)
+            GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh,
+                                   g.plan.need_tree ? ctx->last_tree.perm : nullptr));
+    }
+    if (cfg->do_potential) {
+        const double pf = cfg->potentfact != 0.0 ? cfg->potentfact : physics().potentfact;
+        PotentialParams pp = potential_params(cfg->theta2, cfg->ndirect, pf, cfg->add_bg);
+        GF_TRY(launch_self_potential(ctx, ctx->last_tree, b->pstart, pp, o->penergy, o->phi, nullptr));
+    }
+    return GF_OK;
+}
+
+void release_graph(StageGraph &g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g.exec = nullptr;
+    g.graph = nullptr;
+}
+
+// Plans with an eager run (whose outputs are the batch's results), runs the
+// fixed-shape pass once uncaptured (it reserves every buffer), then captures.
+int capture_graph(StageGraph &g) {
+    gf_ctx *ctx = g.ctx;
+    release_graph(g);
+    g.plan = StagePlan();
+    GF_TRY(stage_run_locked(ctx, &g.b, &g.cfg, &g.o, nullptr, &g.plan));
+    if (g.plan.onchip) {
+        set_status(GF_ENOTIMPL, "a stage graph does not capture on-chip meshes (mesh_onchip)");
+        return GF_ENOTIMPL;
+    }
+    g.fixed.levels = g.plan.tree.levels + 2;
+    g.fixed.ncap = g.plan.tree.ncap + g.plan.tree.ncap / 4 + 64;
+    const int32_t nh = g.b.nhalo;
+    GF_TRY(g.planned.reserve(sizeof(gf_mesh_desc) * (size_t)std::max(nh, 1)));
+    if (nh > 0 && g.cfg.do_mesh)
+        GF_CUDA_TRY(cudaMemcpy(g.planned.ptr, g.plan.mesh.data(), sizeof(gf_mesh_desc) * nh, cudaMemcpyHostToDevice));
+    if (g.cfg.do_mesh) {
+        GF_TRY(smooth_plan(nh, g.plan.mesh.data(), nullptr, &g.smooth));
+        GF_TRY(g.smooth_blob.reserve(std::max<size_t>(g.smooth.blob.size(), 256)));
+        if (!g.smooth.blob.empty())
+            GF_CUDA_TRY(cudaMemcpy(g.smooth_blob.ptr, g.smooth.blob.data(), g.smooth.blob.size(),
+                                   cudaMemcpyHostToDevice));
+    }
+    GF_TRY(stage_pass_graph(g));
+    GF_TRY(check_device_errors(ctx));
+    g.bufs = context_buffers(ctx);
+    GF_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int st = stage_pass_graph(g);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st != GF_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) {
+        set_status(GF_EDEVICE, "stage graph capture: %s", cudaGetErrorString(ce));
+        return GF_EDEVICE;
+    }
+    g.graph = graph;
+    GF_CUDA_TRY(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    if (context_buffers(ctx) != g.bufs) {  // a buffer grew during capture: the graph holds stale pointers
+        set_status(GF_EDEVICE, "stage graph capture reallocated a scratch buffer");
+        return GF_EDEVICE;
+    }
+    return GF_OK;
+}
+
+}  // namespace
+
+}  // namespace gf
+
+struct gf_stage_graph : gf::StageGraph {};
+
+extern "C" {
+
+int gf_stage_graph_create(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *o,
+                          gf_stage_graph **out) {
+    clear_status();
+    if (!ctx || !b || !cfg || !o || !out || b->nhalo < 0 || b->nparticle < 0) return GF_EINVAL;
+    if (b->nparticle > 0 && (!b->pstart || !b->x || !b->y || !b->z || !b->mass)) return GF_EINVAL;
+    if (cfg->plain_fp64 || cfg->mesh_onchip) {
+        set_status(GF_ENOTIMPL, "a stage graph captures the batched FP32 stage with device-memory meshes");
+        return GF_ENOTIMPL;
+    }
+    *out = nullptr;
+    auto *g = new gf_stage_graph();
+    g->ctx = ctx;
+    g->b = *b;
+    g->cfg = *cfg;
+    g->o = *o;
+    std::lock_guard<std::mutex> lk(ctx->lock);
+    const int st = capture_graph(*g);
+    if (st != GF_OK) {
+        release_graph(*g);
+        delete g;
+        return st;
+    }
+    *out = g;
+    return GF_OK;
+}
+
+int gf_stage_graph_launch(gf_stage_graph *g) {
+    clear_status();
+    if (!g || !g->exec) return GF_EINVAL;
+    std::lock_guard<std::mutex> lk(g->ctx->lock);
+    if (context_buffers(g->ctx) != g->bufs) {
+        set_status(GF_ESTALE, "the context's scratch buffers moved since the capture");
+        return GF_ESTALE;
+    }
+    GF_CUDA_TRY(cudaGraphLaunch(g->exec, g->ctx->stream));
+    return GF_OK;
+}
+
+int gf_stage_graph_sync(gf_stage_graph *g) {
+    clear_status();
+    if (!g) return GF_EINVAL;
+    std::lock_guard<std::mutex> lk(g->ctx->lock);
+    return check_device_errors(g->ctx);
+}
+
+int gf_stage_graph_run(gf_stage_graph *g, int32_t *replanned) {
+    if (replanned) *replanned = 0;
+    int st = gf_stage_graph_launch(g);
+    if (st == GF_OK) st = gf_stage_graph_sync(g);
+    if (st != GF_ESTALE) return st;
+    clear_status();
+    std::lock_guard<std::mutex> lk(g->ctx->lock);
+    g->replans++;
+    if (replanned) *replanned = 1;
+    return capture_graph(*g);  // its eager run leaves this batch's results
+}
+
+int gf_stage_graph_replans(const gf_stage_graph *g) { return g ? g->replans : -1; }
+
+int gf_stage_graph_nodes(const gf_stage_graph *g, int32_t *kernels, int32_t *nodes) {
+    clear_status();
+    if (!g || !g->graph) return GF_EINVAL;
+    size_t n = 0;
+    GF_CUDA_TRY(cudaGraphGetNodes(g->graph, nullptr, &n));
+    std::vector<cudaGraphNode_t> v(n);
+    GF_CUDA_TRY(cudaGraphGetNodes(g->graph, v.data(), &n));
+    int32_t k = 0;
+    for (cudaGraphNode_t nd : v) {
+        cudaGraphNodeType t;
+        GF_CUDA_TRY(cudaGraphNodeGetType(nd, &t));
+        k += t == cudaGraphNodeTypeKernel;
+    }
+    if (kernels) *kernels = k;
+    if (nodes) *nodes = (int32_t)n;
+    return GF_OK;
+}
+
+void gf_stage_graph_destroy(gf_stage_graph *g) {
+    if (!g) return;
+    {
+        std::lock_guard<std::mutex> lk(g->ctx->lock);
+        cudaStreamSynchronize(g->ctx->stream);
+        release_graph(*g);
+    }
+    delete g;
 }
 
 }  // extern "C"

@@ -54,7 +54,24 @@ struct Build {
     int32_t *sub, *pre;             // subtree size, preorder index
     int32_t *par;                   // BFS id of the parent, -1 for roots
     int32_t *counter;               // [0] nodes allocated, [1] overflow flag
+    int32_t *lev;                   // level L holds BFS nodes [lev[L], lev[L+1])
 };
+
+constexpr int kMaxLevels = 4096;
+
+// Grid-stride range of the nodes of level L (bounds in device memory).
+#define FOR_LEVEL_NODES(node, L, b)                                                          \
+    for (int node = (b).lev[L] + blockIdx.x * blockDim.x + threadIdx.x; node < (b).lev[(L) + 1]; \
+         node += gridDim.x * blockDim.x)
+
+__global__ void init_build(int32_t nhalo, Build b) {
+    if (threadIdx.x == 0) {
+        b.counter[0] = nhalo;  // the roots are nodes 0 .. nhalo-1
+        b.counter[1] = 0;
+        b.lev[0] = 0;
+        b.lev[1] = nhalo;
+    }
+}
 
 __global__ void init_roots(int32_t nhalo, const int64_t *__restrict__ pstart, Build b) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
@@ -145,14 +162,14 @@ accum_mass(int64_t n, const float4 *__restrict__ pos, const int32_t *__restrict_
     }
 }
 
-__global__ void finalize_com(int32_t lvl0, int32_t lvl1, Build b) {
-    int node = lvl0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= lvl1) return;
-    const double m = b.m[node];
-    if (m > 0) {  // ost.c:553-555
-        b.mx[node] /= m;
-        b.my[node] /= m;
-        b.mz[node] /= m;
+__global__ void finalize_com(int L, Build b) {
+    FOR_LEVEL_NODES(node, L, b) {
+        const double m = b.m[node];
+        if (m > 0) {  // ost.c:553-555
+            b.mx[node] /= m;
+            b.my[node] /= m;
+            b.mz[node] /= m;
+        }
     }
 }
 
@@ -236,9 +253,11 @@ accum_moments(int64_t n, const float4 *__restrict__ pos, const int32_t *__restri
 }
 
 // Decides children, allocates them, and lays out [loose | children] ranges.
-__global__ void split_nodes(int32_t lvl0, int32_t lvl1, int32_t ncap, Build b) {
-    int node = lvl0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= lvl1) return;
+// last: the final level of a fixed-depth build, whose nodes keep all their
+// particles loose (children there would never be processed); a node that
+// would have split flags the build (counter[1]) instead.
+__global__ void split_nodes(int L, int32_t ncap, int last, Build b) {
+    FOR_LEVEL_NODES(node, L, b) {
     const float r2 = __uint_as_float(b.r2[node]);
     const double nodesize = sqrt((double)r2);           // ost.c:574
     const bool divide = nodesize > 0.5 * kMinWidth;     // divideThisNode, tree.h:36
@@ -247,11 +266,15 @@ __global__ void split_nodes(int32_t lvl0, int32_t lvl1, int32_t ncap, Build b) {
         cnt[c] = b.oct[8 * (int64_t)node + c];
         if (divide && cnt[c] >= kMinCell) nch++;
     }
+    if (last && nch > 0) {
+        atomicOr(b.counter + 1, 2);
+        nch = 0;
+    }
     int first = -1;
     if (nch > 0) {
         first = atomicAdd(b.counter, nch);
         if (first + nch > ncap) {  // out of node capacity: keep all particles loose
-            atomicExch(b.counter + 1, 1);
+            atomicOr(b.counter + 1, 1);
             nch = 0;
             first = -1;
         }
@@ -283,6 +306,12 @@ __global__ void split_nodes(int32_t lvl0, int32_t lvl1, int32_t ncap, Build b) {
     }
     b.first[node] = first;
     b.nchild[node] = nch;
+    }
+}
+
+// The next level: the nodes allocated by split_nodes of level L.
+__global__ void close_level(int L, int32_t ncap, Build b) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) b.lev[L + 2] = min(b.counter[0], ncap);
 }
 
 __global__ void scatter_particles(int64_t n, const float4 *__restrict__ pos_in,
@@ -316,31 +345,61 @@ __global__ void scatter_particles(int64_t n, const float4 *__restrict__ pos_in,
 }
 
 // subtree sizes, deepest level first
-__global__ void subtree_sizes(int32_t lvl0, int32_t lvl1, Build b) {
-    int node = lvl0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= lvl1) return;
-    int s = 1;
-    const int f = b.first[node];
-    for (int c = 0; c < b.nchild[node]; c++) s += b.sub[f + c];
-    b.sub[node] = s;
-}
-
-// preorder numbers, shallowest level first (roots set beforehand)
-__global__ void preorder(int32_t lvl0, int32_t lvl1, Build b) {
-    int node = lvl0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= lvl1) return;
-    int p = b.pre[node] + 1;
-    const int f = b.first[node];
-    for (int c = 0; c < b.nchild[node]; c++) {
-        b.pre[f + c] = p;
-        p += b.sub[f + c];
+__global__ void subtree_sizes(int L, Build b) {
+    FOR_LEVEL_NODES(node, L, b) {
+        int s = 1;
+        const int f = b.first[node];
+        for (int c = 0; c < b.nchild[node]; c++) s += b.sub[f + c];
+        b.sub[node] = s;
     }
 }
 
-__global__ void emit_nodes(int32_t nnode, float theta2, Build b, KnnNode *__restrict__ knn,
+// Preorder numbers of the roots: consecutive blocks in halo order (an
+// exclusive scan of the roots' subtree sizes, one block).
+__global__ void __launch_bounds__(1024) root_preorder(int32_t nhalo, Build b) {
+    __shared__ int32_t part[1024];
+    const int t = threadIdx.x;
+    const int per = (nhalo + 1023) / 1024;
+    const int h0 = min(nhalo, t * per), h1 = min(nhalo, h0 + per);
+    int32_t sum = 0;
+    for (int h = h0; h < h1; h++) sum += b.sub[h];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan
+        const int32_t v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int32_t acc = part[t] - sum;
+    for (int h = h0; h < h1; h++) {
+        b.pre[h] = acc;
+        acc += b.sub[h];
+    }
+}
+
+// Flags a fixed-depth build that the batch outgrew: a node of the last level
+// that would have split, or the node capacity exceeded.  The tree built is
+// consistent either way (those particles stay loose).
+__global__ void check_build(Build b, int *err) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && b.counter[1]) atomicOr(err, GF_ERRBIT_PLAN);
+}
+
+// preorder numbers, shallowest level first (roots set beforehand)
+__global__ void preorder(int L, Build b) {
+    FOR_LEVEL_NODES(node, L, b) {
+        int p = b.pre[node] + 1;
+        const int f = b.first[node];
+        for (int c = 0; c < b.nchild[node]; c++) {
+            b.pre[f + c] = p;
+            p += b.sub[f + c];
+        }
+    }
+}
+
+__global__ void emit_nodes(int nlev, float theta2, Build b, KnnNode *__restrict__ knn,
                            BhNode *__restrict__ bh, int32_t *__restrict__ owner) {
-    int node = blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= nnode) return;
+    for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < b.lev[nlev]; node += gridDim.x * blockDim.x) {
     const int i = b.pre[node];
     KnnNode k;
     for (int a = 0; a < 3; a++) {
@@ -371,6 +430,7 @@ __global__ void emit_nodes(int32_t nnode, float theta2, Build b, KnnNode *__rest
     h.lcount = k.lcount;
     h.count = k.count;
     bh[i] = h;
+    }
 }
 
 __global__ void emit_roots(int32_t nhalo, Build b, int32_t *__restrict__ root,
@@ -409,13 +469,19 @@ T *carve(char *&p, size_t count) {
 }  // namespace
 
 int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
-               const float4 *pos_in, float theta2, int q5_asbuilt, TreeView *out) {
+               const float4 *pos_in, float theta2, int q5_asbuilt, TreeView *out,
+               const TreeShape *fixed, TreeShape *shape) {
     if (n > 0x7fffffffLL) {
         set_status(GF_ENOTIMPL, "tree build over more than 2^31 particles in one batch");
         return GF_ENOTIMPL;
     }
-    int64_t ncap = n / 2 + 2LL * nhalo + 1024;
-    for (int attempt = 0; attempt < 4; attempt++, ncap *= 2) {
+    if (fixed && (fixed->levels < 1 || fixed->levels > kMaxLevels || fixed->ncap < nhalo)) {
+        set_status(GF_EINVAL, "fixed tree shape: %d levels, %lld nodes", fixed ? fixed->levels : 0,
+                   fixed ? (long long)fixed->ncap : 0LL);
+        return GF_EINVAL;
+    }
+    int64_t ncap = fixed ? fixed->ncap : n / 2 + 2LL * nhalo + 1024;
+    for (int attempt = 0; attempt < (fixed ? 1 : 4); attempt++, ncap *= 2) {
         // ---- particle buffers: pos x2, perm x2, pnode x2, key
         auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
         const size_t pbytes = 2 * al(n * sizeof(float4)) + 4 * al(n * sizeof(int32_t)) + al(n);
@@ -428,7 +494,8 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         // ---- node buffers (BFS numbering): exactly the carves below
         const size_t nc = (size_t)ncap;
         const size_t nbytes = 3 * al(nc * 4) + 4 * al(nc * 8) + al(nc * 4) + al(nc * 24) +
-                              al(nc * 24) + 3 * al(nc * 32) + 7 * al(nc * 4) + al(64);
+                              al(nc * 24) + 3 * al(nc * 32) + 7 * al(nc * 4) + al(64) +
+                              al((kMaxLevels + 2) * sizeof(int32_t));
         GF_TRY(ctx->tree[1].reserve(nbytes + 256));
         char *np_ = ctx->tree[1].as<char>();
         Build b;
@@ -456,6 +523,7 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         b.pre = carve<int32_t>(np_, nc);
         b.par = carve<int32_t>(np_, nc);
         b.counter = carve<int32_t>(np_, 16);
+        b.lev = carve<int32_t>(np_, kMaxLevels + 2);
         cudaStream_t s = ctx->stream;
         GF_CUDA_TRY(cudaMemsetAsync(zero_begin, 0, zero_end - zero_begin, s));
         // box: minima start at all-ones, maxima at zero (per node: 3 min then 3 max)
@@ -465,10 +533,8 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
             // min slots set to 0xff..: strided pattern, do it with a 2D memset
             GF_CUDA_TRY(cudaMemset2DAsync(b.box, 6 * 4, 0xff, 3 * 4, nc, s));
         }
-        int32_t init_counter[2] = {nhalo, 0};
-        GF_CUDA_TRY(cudaMemcpyAsync(b.counter, init_counter, sizeof(init_counter),
-                                    cudaMemcpyHostToDevice, s));
-        GF_CUDA_TRY(cudaStreamSynchronize(s));  // init_counter is a stack array
+        init_build<<<1, 32, 0, s>>>(nhalo, b);
+        GF_LAUNCH_CHECK();
         if (nhalo > 0) {
             init_roots<<<grid_exact(nhalo, 256), 256, 0, s>>>(nhalo, pstart_dev, b);
             GF_LAUNCH_CHECK();
@@ -476,75 +542,84 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         init_particles<<<grid_n(n), kBlock, 0, s>>>(n, pstart_dev, nhalo, pos_in, pos[0], perm[0],
                                                     pnode[0]);
         GF_LAUNCH_CHECK();
-        std::vector<int32_t> levels = {0, nhalo};
+        // Level by level.  Eagerly, the node count is read back after each
+        // level and the build stops at the first level that allocates no
+        // children; with a fixed shape it runs fixed->levels levels without
+        // a host round trip (the levels past the tree's depth are empty: their
+        // particle passes copy settled particles through) and check_build
+        // flags a tree that needed more levels or nodes.
+        const int fixed_grid = sm_count() * 4;
+        std::vector<int32_t> levels = {0, nhalo};  // eager only: the host copy of b.lev
         int cur = 0;
         int32_t hc[2] = {nhalo, 0};
-        while (levels[levels.size() - 2] < levels.back()) {
-            const int32_t l0 = levels[levels.size() - 2], l1 = levels.back();
+        int nlev = 0;
+        for (int L = 0; fixed ? L < fixed->levels : levels[L] < levels[L + 1]; L++) {
+            const int gl = fixed ? fixed_grid : grid_exact(levels[L + 1] - levels[L], 256);
             accum_mass<<<grid_n(n), kBlock, 0, s>>>(n, pos[cur], pnode[cur], b);
             GF_LAUNCH_CHECK();
-            finalize_com<<<grid_exact(l1 - l0, 256), 256, 0, s>>>(l0, l1, b);
+            finalize_com<<<gl, 256, 0, s>>>(L, b);
             GF_LAUNCH_CHECK();
             accum_moments<<<grid_n(n), kBlock, 0, s>>>(n, pos[cur], pnode[cur], pkey, q5_asbuilt, b);
             GF_LAUNCH_CHECK();
-            split_nodes<<<grid_exact(l1 - l0, 256), 256, 0, s>>>(l0, l1, (int32_t)ncap, b);
+            split_nodes<<<gl, 256, 0, s>>>(L, (int32_t)ncap, fixed && L == fixed->levels - 1, b);
             GF_LAUNCH_CHECK();
             scatter_particles<<<grid_n(n), kBlock, 0, s>>>(n, pos[cur], perm[cur], pnode[cur], pkey,
                                                            pos[cur ^ 1], perm[cur ^ 1],
                                                            pnode[cur ^ 1], b);
             GF_LAUNCH_CHECK();
+            close_level<<<1, 32, 0, s>>>(L, (int32_t)ncap, b);
+            GF_LAUNCH_CHECK();
             cur ^= 1;
+            nlev = L + 1;
+            if (fixed) continue;
             GF_CUDA_TRY(cudaMemcpyAsync(hc, b.counter, sizeof(hc), cudaMemcpyDeviceToHost, s));
             GF_CUDA_TRY(cudaStreamSynchronize(s));
             if (hc[1]) break;
             levels.push_back(std::min<int32_t>(hc[0], (int32_t)ncap));
-            if (levels.size() > 4096) {
-                set_status(GF_EINVAL, "octree deeper than 4096 levels");
+            if (levels.size() > (size_t)kMaxLevels) {
+                set_status(GF_EINVAL, "octree deeper than %d levels", kMaxLevels);
                 return GF_EINVAL;
             }
         }
         if (hc[1]) continue;  // node capacity exceeded: retry with more nodes
-        const int32_t nnode = levels.back();
-        const int nlev = (int)levels.size() - 1;
-        for (int L = nlev - 1; L >= 0; L--) {
-            subtree_sizes<<<grid_exact(levels[L + 1] - levels[L], 256), 256, 0, s>>>(levels[L],
-                                                                                  levels[L + 1], b);
+        if (fixed) {
+            check_build<<<1, 32, 0, s>>>(b, ctx->d_err);
             GF_LAUNCH_CHECK();
         }
-        // roots: consecutive preorder blocks in halo order
-        std::vector<int32_t> sub(std::max(nhalo, 1)), pre(std::max(nhalo, 1));
+        const int32_t nnode = fixed ? -1 : levels.back();
+        for (int L = nlev - 1; L >= 0; L--) {
+            subtree_sizes<<<fixed ? fixed_grid : grid_exact(levels[L + 1] - levels[L], 256), 256, 0, s>>>(L, b);
+            GF_LAUNCH_CHECK();
+        }
         if (nhalo > 0) {
-            GF_CUDA_TRY(cudaMemcpyAsync(sub.data(), b.sub, sizeof(int32_t) * nhalo,
-                                        cudaMemcpyDeviceToHost, s));
-            GF_CUDA_TRY(cudaStreamSynchronize(s));
-            int32_t acc0 = 0;
-            for (int h = 0; h < nhalo; h++) {
-                pre[h] = acc0;
-                acc0 += sub[h];
-            }
-            GF_CUDA_TRY(cudaMemcpyAsync(b.pre, pre.data(), sizeof(int32_t) * nhalo,
-                                        cudaMemcpyHostToDevice, s));
+            root_preorder<<<1, 1024, 0, s>>>(nhalo, b);
+            GF_LAUNCH_CHECK();
         }
         for (int L = 0; L < nlev; L++) {
-            preorder<<<grid_exact(levels[L + 1] - levels[L], 256), 256, 0, s>>>(levels[L],
-                                                                             levels[L + 1], b);
+            preorder<<<fixed ? fixed_grid : grid_exact(levels[L + 1] - levels[L], 256), 256, 0, s>>>(L, b);
             GF_LAUNCH_CHECK();
         }
+        if (shape) {
+            shape->levels = nlev;
+            shape->ncap = ncap;
+            shape->nnode = nnode;
+        }
         // ---- output buffers
-        const size_t obytes = al((size_t)std::max(nnode, 1) * sizeof(KnnNode)) +
-                              al((size_t)std::max(nnode, 1) * sizeof(BhNode)) +
+        const int64_t nout = fixed ? ncap : std::max(nnode, 1);  // node slots written
+        const size_t obytes = al((size_t)nout * sizeof(KnnNode)) + al((size_t)nout * sizeof(BhNode)) +
                               2 * al((size_t)std::max(nhalo, 1) * 4) +
                               2 * al((size_t)std::max<int64_t>(n, 1) * 4);
         GF_TRY(ctx->tree[2].reserve(obytes + 256));
         char *op = ctx->tree[2].as<char>();
-        KnnNode *knn = carve<KnnNode>(op, std::max(nnode, 1));
-        BhNode *bh = carve<BhNode>(op, std::max(nnode, 1));
+        KnnNode *knn = carve<KnnNode>(op, (size_t)nout);
+        BhNode *bh = carve<BhNode>(op, (size_t)nout);
         int32_t *root = carve<int32_t>(op, std::max(nhalo, 1));
         int32_t *rend = carve<int32_t>(op, std::max(nhalo, 1));
         int32_t *phalo = carve<int32_t>(op, std::max<int64_t>(n, 1));
         int32_t *owner = carve<int32_t>(op, std::max<int64_t>(n, 1));
-        if (nnode > 0) {
-            emit_nodes<<<grid_exact(nnode, 256), 256, 0, s>>>(nnode, theta2, b, knn, bh, owner);
+        if (fixed || nnode > 0) {
+            emit_nodes<<<fixed ? fixed_grid : grid_exact(nnode, 256), 256, 0, s>>>(nlev, theta2, b, knn, bh,
+                                                                                  owner);
             GF_LAUNCH_CHECK();
             emit_roots<<<grid_exact(nhalo, 256), 256, 0, s>>>(nhalo, b, root, rend);
             GF_LAUNCH_CHECK();

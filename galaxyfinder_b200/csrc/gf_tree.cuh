@@ -10,8 +10,29 @@ namespace gf {
 // theta2 fills BhNode::open_r2; q5_asbuilt reproduces ost.c:571 (m*y*x in
 // place of m*y*z).  Buffers live in ctx->tree[]; the view stays valid until
 // the next build on ctx.
+// Shape of a built octree: levels processed, node capacity and node count
+// (-1 for a build with a fixed shape, whose count stays on the device).
+struct TreeShape {
+    int32_t levels = 0;
+    int64_t ncap = 0;
+    int32_t nnode = 0;
+};
+// What a captured stage pass takes from an eager run of the stage.
+struct StagePlan {
+    bool need_tree = false, onchip = false;
+    std::vector<gf_mesh_desc> mesh;  // planned meshes (offsets into the mesh buffer)
+    int64_t cells = 0, dev_cells = 0;
+    TreeShape tree;                  // the octree the eager run built
+};
+int stage_run_locked(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *o,
+                     gf_stage_stats *st, StagePlan *plan);
+
+// With `fixed`, the build runs fixed->levels levels over fixed->ncap node
+// slots with no host round trip (capturable in a CUDA graph) and flags
+// GF_ERRBIT_PLAN when the batch needs more; `shape` receives the shape built.
 int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
-               const float4 *pos, float theta2, int q5_asbuilt, TreeView *out);
+               const float4 *pos, float theta2, int q5_asbuilt, TreeView *out,
+               const TreeShape *fixed = nullptr, TreeShape *shape = nullptr);
 
 // Potential walk parameters (see gf_potent.cu).
 struct PotentialParams {

@@ -39,6 +39,7 @@ extern "C" {
 #define GF_ETIMEOUT 4  /* a device-side bounded wait gave up */
 #define GF_ERANGE 5    /* a particle fell outside its mesh (the reference would write out of bounds) */
 #define GF_ENOTIMPL 6
+#define GF_ESTALE 7    /* a captured stage graph's plan no longer fits the batch: re-plan */
 
 const char *gf_status_string(int status);
 /* Status and message of the most recent call made by this host thread. */
@@ -51,8 +52,10 @@ int gf_set_device(int device);
  * must prove the GPU path ran). */
 uint64_t gf_kernel_launch_count(void);
 /* Compile-time launch parameter `name` of the loaded library (GF_KNN_ALGO,
- * GF_KNNB_BLOCK, GF_KNNB_ARITY, GF_KNNB_SEEDS, GF_KNN_BLOCK, GF_KNN_MINB, GF_KNN_CHUNK,
- * GF_BH_BLOCK, GF_BH_MINB, GF_FFT_PENCILS, GF_TREE_BLOCK) in *value.
+ * GF_KNNB_BLOCK, GF_KNNB_ARITY, GF_KNNB_SEEDS, GF_KNNB_QUEUE, GF_KNNB_LANECERT,
+ * GF_KNN_BLOCK, GF_KNN_MINB, GF_KNN_CHUNK, GF_BH_BLOCK, GF_BH_MINB, GF_BH_ALGO,
+ * GF_FFT_PENCILS, GF_FFT_PENCILS_64, GF_FFT_PENCILS_128, GF_TSC_TILE,
+ * GF_TREE_BLOCK) in *value.
  * Returns GF_EINVAL for an unknown name. */
 int gf_tuning_value(const char *name, int64_t *value);
 
@@ -443,6 +446,37 @@ typedef struct gf_stage_stats {
 /* stats may be NULL; when given, per-phase CUDA-event times are filled in. */
 int gf_stage_run(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *out,
                  gf_stage_stats *stats);
+
+/* The stage captured as one CUDA graph on ctx's stream (no reference
+ * counterpart: the reference runs the stage per halo on the host).
+ * gf_stage_graph_create runs gf_stage_run once to plan (the meshes from the
+ * halo extents, the octree's depth and node count; its outputs are this
+ * batch's results), then captures a pass that computes the frames and meshes
+ * on the device, builds the octree with a fixed depth (two levels above the
+ * planned one) and node capacity (a quarter above), and runs every kernel of
+ * the stage with no host round trip.  The batch, config and output structs
+ * are copied: the device buffers they point to must stay allocated and are
+ * read and written by every replay.
+ *
+ * gf_stage_graph_launch replays the graph asynchronously on the batch's
+ * current contents; gf_stage_graph_sync waits and reports GF_ESTALE when a
+ * replay no longer fitted the plan (a mesh changed shape or the octree
+ * outgrew the fixed depth or capacity: its outputs are then not valid) or
+ * when the context's scratch buffers moved (another call on ctx needed more).
+ * gf_stage_graph_run launches, waits and, on GF_ESTALE, re-plans and
+ * re-captures (the eager planning run leaves valid outputs) and sets
+ * *replanned.  Graphs capture the batched FP32 stage with device-memory
+ * meshes (GF_ENOTIMPL for plain_fp64 or mesh_onchip); stats are not kept. */
+typedef struct gf_stage_graph gf_stage_graph;
+int gf_stage_graph_create(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg, gf_stage_out *out,
+                          gf_stage_graph **graph);
+int gf_stage_graph_launch(gf_stage_graph *graph);
+int gf_stage_graph_sync(gf_stage_graph *graph);
+int gf_stage_graph_run(gf_stage_graph *graph, int32_t *replanned);
+int gf_stage_graph_replans(const gf_stage_graph *graph);
+/* Kernel nodes and all nodes of the captured graph. */
+int gf_stage_graph_nodes(const gf_stage_graph *graph, int32_t *kernels, int32_t *nodes);
+void gf_stage_graph_destroy(gf_stage_graph *graph);
 
 #ifdef __cplusplus
 }
