@@ -227,6 +227,9 @@ SIGNATURES = {
     "gf_stage_graph_create": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),
                                      ctypes.POINTER(StageOut), ctypes.POINTER(_VP)]),
     "gf_stage_graph_launch": (_INT, [_VP]),
+    "gf_bound_pass": (_INT, [_VP, _INT, _VP, _VP, _VP, _INT, _VP, _VP, _INT, _VP, _VP]),
+    "gf_shell_bound": (_INT, [_VP, _INT, _VP, _VP, _VP, _VP, _VP, _VP, _INT, _INT, _VP, _INT, _VP, _INT, _VP,
+                              _VP]),
     "gf_stage_graph_sync": (_INT, [_VP]),
     "gf_stage_graph_run": (_INT, [_VP, ctypes.POINTER(_I32)]),
     "gf_stage_graph_replans": (_INT, [_VP]),

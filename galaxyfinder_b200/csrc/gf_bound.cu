@@ -50,65 +50,6 @@ __global__ void energy_flag_kernel(int n, const double *__restrict__ r, const fl
     if ((threadIdx.x & 31) == 0) atomicAdd(nbound, local);
 }
 
-int energy_check(const Kptype *tkp, int tnp, unsigned char *bndflag, const Kptype *skp, int snp,
-                 bool self, const double c[6]) {
-    gf_ctx *ctx = default_ctx();
-    if (!ctx) return -1;
-    std::lock_guard<std::mutex> g(ctx->lock);
-    std::vector<Vector3d> tr((size_t)tnp), sr;
-    std::vector<float> v(3 * (size_t)tnp), smass;
-    for (int i = 0; i < tnp; i++) {
-        tr[i].x = tkp[i].x;
-        tr[i].y = tkp[i].y;
-        tr[i].z = tkp[i].z;
-        v[3 * i] = tkp[i].vx;
-        v[3 * i + 1] = tkp[i].vy;
-        v[3 * i + 2] = tkp[i].vz;
-    }
-    const Kptype *src = self ? tkp : skp;
-    const int ns = self ? tnp : snp;
-    sr.resize((size_t)ns);
-    smass.resize((size_t)ns);
-    for (int i = 0; i < ns; i++) {
-        sr[i].x = src[i].x;
-        sr[i].y = src[i].y;
-        sr[i].z = src[i].z;
-        smass[i] = src[i].mass;
-    }
-    float *dpe = nullptr;
-    const double *dr = nullptr;
-    if (potent_device(ctx, tnp, tr.data(), ns, sr.data(), smass.data(), self, &dpe, &dr) != GF_OK)
-        return -1;
-    const size_t vbytes = 3 * (size_t)tnp * sizeof(float);
-    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-    if (ctx->tmp[1].reserve(al(vbytes) + al((size_t)tnp) + 256) != GF_OK) return -1;
-    float *dv = ctx->tmp[1].as<float>();
-    unsigned char *dflag = ctx->tmp[1].as<unsigned char>() + al(vbytes);
-    int *dcount = reinterpret_cast<int *>(dflag + al((size_t)tnp));
-    if (cudaMemcpyAsync(dv, v.data(), vbytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
-        cudaMemsetAsync(dcount, 0, sizeof(int), ctx->stream) != cudaSuccess) {
-        set_status(GF_EDEVICE, "energy check: copy failed");
-        return -1;
-    }
-    const gf_physics &ph = physics();
-    energy_flag_kernel<<<grid_for(tnp), 256, 0, ctx->stream>>>(
-        tnp, dr, dv, dpe, c[0], c[1], c[2], c[3], c[4], c[5], ph.r1kineticfact, ph.r2kineticfact,
-        dflag, dcount);
-    count_launch();
-    if (cudaGetLastError() != cudaSuccess) {
-        set_status(GF_EDEVICE, "energy check: launch failed");
-        return -1;
-    }
-    int nbound = 0;
-    if (cudaMemcpyAsync(bndflag, dflag, (size_t)tnp, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-        cudaMemcpyAsync(&nbound, dcount, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) {
-        set_status(GF_EDEVICE, "energy check: copy back failed");
-        return -1;
-    }
-    if (check_device_errors(ctx) != GF_OK) return -1;
-    return nbound;
-}
-
 // ------------------------------------------------------------------ tidal radius
 constexpr double kMaxTidalR = 2.e5;  // MAX_TIDAL_R, subhaloden.mod6.c:34
 constexpr int kNumMass = 10000;      // NUM_MASS, header.h:97
@@ -254,6 +195,65 @@ __global__ void tidal_compact_kernel(int n, const int32_t *__restrict__ plist,
 }
 
 }  // namespace
+
+int energy_check(const Kptype *tkp, int tnp, unsigned char *bndflag, const Kptype *skp, int snp,
+                 bool self, const double c[6]) {
+    gf_ctx *ctx = default_ctx();
+    if (!ctx) return -1;
+    std::lock_guard<std::mutex> g(ctx->lock);
+    std::vector<Vector3d> tr((size_t)tnp), sr;
+    std::vector<float> v(3 * (size_t)tnp), smass;
+    for (int i = 0; i < tnp; i++) {
+        tr[i].x = tkp[i].x;
+        tr[i].y = tkp[i].y;
+        tr[i].z = tkp[i].z;
+        v[3 * i] = tkp[i].vx;
+        v[3 * i + 1] = tkp[i].vy;
+        v[3 * i + 2] = tkp[i].vz;
+    }
+    const Kptype *src = self ? tkp : skp;
+    const int ns = self ? tnp : snp;
+    sr.resize((size_t)ns);
+    smass.resize((size_t)ns);
+    for (int i = 0; i < ns; i++) {
+        sr[i].x = src[i].x;
+        sr[i].y = src[i].y;
+        sr[i].z = src[i].z;
+        smass[i] = src[i].mass;
+    }
+    float *dpe = nullptr;
+    const double *dr = nullptr;
+    if (potent_device(ctx, tnp, tr.data(), ns, sr.data(), smass.data(), self, &dpe, &dr) != GF_OK)
+        return -1;
+    const size_t vbytes = 3 * (size_t)tnp * sizeof(float);
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    if (ctx->tmp[1].reserve(al(vbytes) + al((size_t)tnp) + 256) != GF_OK) return -1;
+    float *dv = ctx->tmp[1].as<float>();
+    unsigned char *dflag = ctx->tmp[1].as<unsigned char>() + al(vbytes);
+    int *dcount = reinterpret_cast<int *>(dflag + al((size_t)tnp));
+    if (cudaMemcpyAsync(dv, v.data(), vbytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(dcount, 0, sizeof(int), ctx->stream) != cudaSuccess) {
+        set_status(GF_EDEVICE, "energy check: copy failed");
+        return -1;
+    }
+    const gf_physics &ph = physics();
+    energy_flag_kernel<<<grid_for(tnp), 256, 0, ctx->stream>>>(
+        tnp, dr, dv, dpe, c[0], c[1], c[2], c[3], c[4], c[5], ph.r1kineticfact, ph.r2kineticfact,
+        dflag, dcount);
+    count_launch();
+    if (cudaGetLastError() != cudaSuccess) {
+        set_status(GF_EDEVICE, "energy check: launch failed");
+        return -1;
+    }
+    int nbound = 0;
+    if (cudaMemcpyAsync(bndflag, dflag, (size_t)tnp, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&nbound, dcount, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) {
+        set_status(GF_EDEVICE, "energy check: copy back failed");
+        return -1;
+    }
+    if (check_device_errors(ctx) != GF_OK) return -1;
+    return nbound;
+}
 
 }  // namespace gf
 

@@ -30,18 +30,6 @@ __global__ void vec3_pos_kernel(int64_t n, const double *__restrict__ r, const f
 
 int grid1(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sm_count() * 16)); }
 
-PotentialParams potential_params(float theta2, int ndirect, double potentfact, int add_bg) {
-    const gf_physics &ph = physics();
-    PotentialParams pp;
-    pp.theta2 = theta2;
-    pp.ndirect = ndirect;
-    pp.potentfact = potentfact;
-    pp.add_bg = add_bg;
-    pp.amax = ph.amax;
-    pp.a = ph.a;
-    pp.omep = ph.omep;
-    return pp;
-}
 
 struct EventTimer {
     cudaStream_t s;
@@ -67,6 +55,19 @@ struct EventTimer {
 };
 
 }  // namespace
+
+PotentialParams potential_params(float theta2, int ndirect, double potentfact, int add_bg) {
+    const gf_physics &ph = physics();
+    PotentialParams pp;
+    pp.theta2 = theta2;
+    pp.ndirect = ndirect;
+    pp.potentfact = potentfact;
+    pp.add_bg = add_bg;
+    pp.amax = ph.amax;
+    pp.a = ph.a;
+    pp.omep = ph.omep;
+    return pp;
+}
 
 }  // namespace gf
 

@@ -17,6 +17,12 @@ struct TreeShape {
     int64_t ncap = 0;
     int32_t nnode = 0;
 };
+// The energy test of CheckSelfTE / CheckExternalTE (gf_bound.cu) on the
+// default context: bndflag per target, the bound count, or -1 with the status
+// set.  c: the centre and velocity of the KE (x, y, z, vx, vy, vz).
+int energy_check(const Kptype *tkp, int tnp, unsigned char *bndflag, const Kptype *skp, int snp, bool self,
+                 const double c[6]);
+
 // What a captured stage pass takes from an eager run of the stage.
 struct StagePlan {
     bool need_tree = false, onchip = false;
@@ -42,6 +48,9 @@ struct PotentialParams {
     int32_t add_bg;       // add the NFW background term of the halo mass
     float amax, a, omep;  // cosmology for the background term
 };
+
+// The walk parameters with the cosmology of the background term (gf_stage.cu).
+PotentialParams potential_params(float theta2, int ndirect, double potentfact, int add_bg);
 
 // pos_batch: the same FP32 positions in batch order (seeds re-read them by
 // batch index).

@@ -126,6 +126,47 @@ def CheckExternalTE(tkp, skp, core):
     return flags, nb
 
 
+def shell_bound(bp, flag, haloid, shellp, shellc, ishell, cores, order):
+    """gf_shell_bound: shell `ishell` of the boundedness loop
+    (subhaloden.mod6.c:3033-3101) batched over its cores.  flag (uint8) and
+    haloid (int32) are updated in place; shellp / shellc are the SHELL2P /
+    SHELL2C lists.  Returns (bound count per core of `order`, cores retested
+    alone)."""
+    bp = np.ascontiguousarray(bp, _lib.BP_DTYPE)
+    assert flag.dtype == np.uint8 and flag.flags.c_contiguous
+    assert haloid.dtype == np.int32 and haloid.flags.c_contiguous
+    sp = np.concatenate([np.asarray(q, np.int32) for q in shellp]) if len(shellp) else np.zeros(0, np.int32)
+    sps = np.concatenate([[0], np.cumsum([len(q) for q in shellp])]).astype(np.int32)
+    sc = np.concatenate([np.asarray(q, np.int32) for q in shellc]) if len(shellc) else np.zeros(0, np.int32)
+    scs = np.concatenate([[0], np.cumsum([len(q) for q in shellc])]).astype(np.int32)
+    cores = np.ascontiguousarray(cores, _lib.CORE_DTYPE)
+    order = np.ascontiguousarray(order, np.int32)
+    nmem = np.zeros(max(len(order), 1), np.int32)
+    nret = np.zeros(1, np.int32)
+    _lib.check(lib().gf_shell_bound(ptr(bp), len(bp), ptr(flag), ptr(haloid), ptr(sp), ptr(sps), ptr(sc), ptr(scs),
+                               len(shellp), ishell, ptr(cores), len(cores), ptr(order), len(order), ptr(nmem),
+                               ptr(nret)))
+    return [int(v) for v in nmem[:len(order)]], int(nret[0])
+
+
+def bound_pass(bp, flag, haloid, cores, order, nmem):
+    """gf_bound_pass: one BOUNDITER pass (subhaloden.mod6.c:3118-3172) over the
+    cores of `order` (nmem: their member counts at the start of the pass),
+    batched.  flag (uint8) and haloid (int32) are updated in place.  Returns
+    (bound count per core of `order`, GPU passes used)."""
+    bp = np.ascontiguousarray(bp, _lib.BP_DTYPE)
+    assert flag.dtype == np.uint8 and flag.flags.c_contiguous
+    assert haloid.dtype == np.int32 and haloid.flags.c_contiguous
+    cores = np.ascontiguousarray(cores, _lib.CORE_DTYPE)
+    order = np.ascontiguousarray(order, np.int32)
+    nmem = np.ascontiguousarray(nmem, np.int32)
+    nb = np.zeros(max(len(order), 1), np.int32)
+    nbatch = np.zeros(1, np.int32)
+    _lib.check(lib().gf_bound_pass(ptr(bp), len(bp), ptr(flag), ptr(haloid), ptr(cores), len(cores), ptr(order),
+                                   ptr(nmem), len(order), ptr(nb), ptr(nbatch)))
+    return [int(v) for v in nb[:len(order)]], int(nbatch[0])
+
+
 def tidal_radius(core, score_core, bp, haloid):
     """AdGetTidalRCenterCore (subhaloden.mod6.c:1910): fills core['Rtidal'] and
     core['nummem'] in place."""

@@ -175,6 +175,44 @@ void i_potent_spline(void);
  * as haloid[np] (negative: no core), and score_core[ncore] lists the core ids
  * in the reference's score order (increasing member count).  Fills
  * core[].Rtidal and core[].nummem.  Host pointers, synchronous. */
+/* One shell of subhalo_den's boundedness loop (subhaloden.mod6.c:3033-3101),
+ * batched over the shell's cores: for each core of `order` (the shell's
+ * cores after the loop's qsort by member count) the shell's particles not yet
+ * bound and every REMAINING particle within the core's Rtidal are tested
+ * against the core's members and the later shells that hold the core
+ * (CheckExternalTE); the bound ones join the core, the others become
+ * REMAINING; then the shell's unbound particles become REMAINING
+ * (UnboundShellP2Rest).  A core's sources do not change during its shell, so
+ * every core's candidates are tested in one GPU pass and the loop is
+ * replayed in the reference's order; a core whose replayed target count
+ * crosses the 1000-target direct-sum bound is retested alone
+ * (*nretest_out counts them).
+ * bp[np]: the halo's particles; flag[np], haloid[np]: wp[].flag (WP_BOUND
+ * 0x10, WP_REMAINING 0x20) and wp[].haloid, updated in place; shellp with
+ * shellp_start[nshell+1] and shellc with shellc_start[nshell+1]: the
+ * SHELL2P and SHELL2C lists; core[numcore] with Rtidal set; nmem_out[norder]
+ * (may be NULL): MULTIHALOSHELL's bound count per core of `order`.  Host
+ * arrays; synchronous. */
+int gf_shell_bound(const SimpleBasicParticleType *bp, int np, unsigned char *flag, int32_t *haloid,
+                   const int32_t *shellp, const int32_t *shellp_start, const int32_t *shellc,
+                   const int32_t *shellc_start, int nshell, int ishell, const Coretype *core, int numcore,
+                   const int32_t *order, int norder, int32_t *nmem_out, int32_t *nretest_out);
+/* One pass of subhalo_den's BOUNDITER loop over the cores
+ * (subhaloden.mod6.c:3118-3172), batched: for each core of `order` (all
+ * cores after the pass's qsort by member count; nmem[] their member counts
+ * at the start of the pass, cores with none skipped; Rtidal set by
+ * gf_tidal_radius) GetMemberRestParticleList and SINGLEHALO (CheckSelfTE:
+ * the list's self potential, the KE about its stellar centre).  The lists
+ * are predicted from the state at the start of a batch and tested in one GPU
+ * pass; the replay in the reference's order keeps a core's result when its
+ * actual list equals the prediction and starts a new batch at the first core
+ * whose list changed (*nbatch_out: GPU passes used).  flag[np] and
+ * haloid[np] (wp[].flag, wp[].haloid) are updated in place; nbound_out[norder]
+ * (may be NULL): SINGLEHALO's bound count per core.  Host arrays;
+ * synchronous. */
+int gf_bound_pass(const SimpleBasicParticleType *bp, int np, unsigned char *flag, int32_t *haloid,
+                  const Coretype *core, int numcore, const int32_t *order, const int32_t *nmem, int norder,
+                  int32_t *nbound_out, int32_t *nbatch_out);
 int gf_tidal_radius(Coretype *core, int numcore, const int32_t *score_core, int ncore,
                     const SimpleBasicParticleType *bp, const int32_t *haloid, int np);
 /* Tidal cut of GetMemberRestParticleList (subhaloden.mod6.c:2734-2745) and
