@@ -330,7 +330,9 @@ int gf_tuning_value(const char *name, int64_t *value) {
                   {"GF_BH_BLOCK", GF_BH_BLOCK},       {"GF_BH_MINB", GF_BH_MINB},
                   {"GF_FFT_PENCILS", GF_FFT_PENCILS}, {"GF_TREE_BLOCK", GF_TREE_BLOCK},
                   {"GF_KNNB_QUEUE", GF_KNNB_QUEUE},   {"GF_KNNB_LANECERT", GF_KNNB_LANECERT},
-                  {"GF_BH_ALGO", GF_BH_ALGO},         {"GF_FFT_PENCILS_64", GF_FFT_PENCILS_64},
+                  {"GF_BH_DYN", GF_BH_DYN},           {"GF_KNNB_DYN", GF_KNNB_DYN},
+                  {"GF_BH_ACC", GF_BH_ACC},
+                  {"GF_FFT_PENCILS_64", GF_FFT_PENCILS_64},
                   {"GF_FFT_PENCILS_128", GF_FFT_PENCILS_128}, {"GF_TSC_TILE", GF_TSC_TILE}};
     if (!name || !value) return GF_EINVAL;
     for (const auto &p : params)
@@ -381,6 +383,7 @@ int gf_ctx_destroy(gf_ctx *c) {
     c->hid.release();
     c->mesh.release();
     c->mesh_boxes.release();
+    c->work.release();
     c->smooth_tables.release();
     c->particles.release();
     for (auto &b : c->tmp) b.release();

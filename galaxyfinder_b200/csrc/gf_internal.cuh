@@ -129,6 +129,7 @@ struct gf_ctx {
     int *d_err = nullptr;  // device error word
     // scratch buffers, named by use
     gf::DevBuf hid, mesh, mesh_boxes, smooth_tables, particles, tmp[8];
+    gf::DevBuf work;  // work counters of the kernels that take their items from a queue
     gf::DevBuf tree[16];
     gf::HostPinned pin[4];
     gf::TreeView last_tree;  // the most recent build_tree() on this context

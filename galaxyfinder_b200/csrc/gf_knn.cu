@@ -784,7 +784,7 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                    const int64_t *__restrict__ pstart, const int32_t *__restrict__ owner,
                    const KnnNode *__restrict__ nodes, int32_t *__restrict__ nearindex,
                    float *__restrict__ dens, int32_t *__restrict__ redo, unsigned *__restrict__ nredo,
-                   unsigned long long *__restrict__ counters) {
+                   unsigned long long *__restrict__ counters, unsigned long long *__restrict__ work) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * kFBucketWarpBytes;
@@ -809,7 +809,14 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t nbucket = (n + 31) >> 5;
-    for (int64_t bucket = wid; bucket < nbucket; bucket += nwarps) {
+    // the warp's next bucket: from the work counter, or grid-stride
+    auto next = [&](int64_t stride_bucket) -> int64_t {
+        if (!GF_KNNB_DYN || !work) return stride_bucket;
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(work, 1ull);
+        return (int64_t)__shfl_sync(0xffffffffu, b, 0);
+    };
+    for (int64_t bucket = next(wid); bucket < nbucket; bucket = next(bucket + nwarps)) {
         const int64_t b = bucket << 5;
         const int64_t q = b + lane;
         const bool valid = q < n;
@@ -1161,8 +1168,14 @@ int launch_knn(gf_ctx *ctx, const TreeView &t, const int64_t *pstart, const floa
         const int64_t nbucket = (t.n + 31) / 32;
         int64_t grid = (nbucket * 32 + block - 1) / block;
         grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)sm_count() * std::max(per_sm, 1)));
+        unsigned long long *work = nullptr;
+        if (GF_KNNB_DYN) {  // one resident wave; each warp takes its next bucket from a counter
+            GF_TRY(ctx->work.reserve(256));
+            work = ctx->work.as<unsigned long long>() + 16;  // slot 16: this search
+            GF_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long), ctx->stream));
+        }
         kern<<<(int)grid, block, shmem, ctx->stream>>>(t.n, k, t.pos, t.perm, pos_batch, t.phalo, pstart, t.owner,
-                                                       t.knn, nearindex, dens, redo, nredo, counters);
+                                                       t.knn, nearindex, dens, redo, nredo, counters, work);
         GF_LAUNCH_CHECK();
         // the uncertified queries, exactly, into their own rows (the count
         // stays on the device; the grid strides over whatever it is)

@@ -26,6 +26,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "gf_tree.cuh"
 
@@ -41,7 +42,18 @@ struct Kahan {
         c = (t - s) - y;
         s = t;
     }
+    __device__ __forceinline__ float value() const { return s + (-c); }
 };
+
+// The sum of a target's FP32 terms: GF_BH_ACC=1 adds them in FP64 (two
+// instructions per term, one dependent add), 0 with FP32 Kahan compensation
+// (four dependent adds); both round once at the end.
+struct Fp64Acc {
+    double s = 0.0;
+    __device__ __forceinline__ void add(float v) { s += (double)v; }
+    __device__ __forceinline__ float value() const { return (float)s; }
+};
+using BhAcc = std::conditional<GF_BH_ACC == 1, Fp64Acc, Kahan>::type;
 
 // GetBGpotent, subhaloden.mod6.c:1059-1101
 __device__ double bg_potent_dev(double mvir, const PotentialParams &pp) {
@@ -62,12 +74,20 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
           const int32_t *__restrict__ root, const int32_t *__restrict__ rend,
           const BhNode *__restrict__ nodes, const int32_t *__restrict__ direct,
           const double *__restrict__ bg, PotentialParams pp, float *__restrict__ out,
-          float *__restrict__ raw, unsigned long long *__restrict__ counters) {
+          float *__restrict__ raw, unsigned long long *__restrict__ counters,
+          unsigned long long *__restrict__ work) {
     const int lane = threadIdx.x & 31;
     const int64_t warp0 = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
     unsigned long long npp = 0, npc = 0;
-    for (int64_t base = warp0; base < ntarget; base += wstride) {
+    // the warp's next 32 targets: from the work counter, or grid-stride
+    auto next = [&](int64_t stride_base) -> int64_t {
+        if (!GF_BH_DYN || !work) return stride_base;
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(work, 32ull);
+        return (int64_t)__shfl_sync(0xffffffffu, b, 0);
+    };
+    for (int64_t base = next(warp0); base < ntarget; base = next(base + wstride)) {
         const int64_t t = base + lane;
         const bool valid = t < ntarget;
         int h = 0, my = INT_MAX, my_end = 0, always_open = 0;
@@ -81,7 +101,7 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
             P = tpos[t];
         }
         const double px = P.x, py = P.y, pz = P.z;
-        Kahan acc;
+        BhAcc acc;
         while (true) {
             const int i = (int)__reduce_min_sync(0xffffffffu, (unsigned)my);
             if (i == INT_MAX) break;
@@ -126,7 +146,7 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
         }
         if (valid) {
             const int64_t o = tout ? tout[t] : t;
-            const float phi = acc.s + (-acc.c);
+            const float phi = acc.value();
             if (raw) raw[o] = phi;
             if (out) {
                 double e = pp.potentfact != 0.0 ? (double)phi * pp.potentfact : (double)phi;
@@ -147,153 +167,27 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
     }
 }
 
-// The same walk and terms with the evaluation taken out of the lockstep walk.
-// The warp's walk (as bh_kernel's: smallest next node of the warp, each lane
-// its own FP64 opening decision) only queues work: an accepted node goes to
-// the lane's cell queue, an opened node with loose particles to its leaf
-// queue (per-lane columns in shared memory).  When a lane's queue is full,
-// and at the end, the warp evaluates: every lane its own cells in step, then
-// every lane its own queued particles one per step (moving to its next leaf
-// as each ends), so the lanes compute terms together instead of waiting for
-// the lanes that share the walk's current node.  Cell and particle terms and
-// the compensated sum are bh_kernel's; only their order differs (cells of a
-// chunk before its particles).
-constexpr int kBhQueue = 32;
-
-__global__ void __launch_bounds__(GF_BH_BLOCK, GF_BH_MINB)
-bh_list_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__restrict__ thalo,
-               const int32_t *__restrict__ tout, const float4 *__restrict__ spos,
-               const int32_t *__restrict__ root, const int32_t *__restrict__ rend,
-               const BhNode *__restrict__ nodes, const int32_t *__restrict__ direct,
-               const double *__restrict__ bg, PotentialParams pp, float *__restrict__ out,
-               float *__restrict__ raw, unsigned long long *__restrict__ counters) {
-    extern __shared__ int32_t bh_queues[];
-    const int lane = threadIdx.x & 31;
-    int32_t *cq = bh_queues + (threadIdx.x >> 5) * (2 * kBhQueue * 32);  // [slot][lane]
-    int32_t *lq = cq + kBhQueue * 32;
-    const int64_t warp0 = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32;
-    const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
-    unsigned long long npp = 0, npc = 0;
-    for (int64_t base = warp0; base < ntarget; base += wstride) {
-        const int64_t t = base + lane;
-        const bool valid = t < ntarget;
-        int h = 0, my = INT_MAX, my_end = 0, always_open = 0;
-        float4 P = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid) {
-            h = thalo[t];
-            my = root[h];
-            my_end = rend[h];
-            if (my >= my_end) my = INT_MAX;
-            always_open = direct ? direct[h] : 0;
-            P = tpos[t];
-        }
-        const double px = P.x, py = P.y, pz = P.z;
-        Kahan acc;
-        int nc = 0, nl = 0;
-        auto flush = [&]() {
-            const int mc = (int)__reduce_max_sync(0xffffffffu, (unsigned)nc);
-            for (int s = 0; s < mc; s++) {
-                if (s < nc) {
-                    const BhNode &nd = nodes[cq[s * 32 + lane]];
-                    const float fx = (float)(px - nd.com[0]);
-                    const float fy = (float)(py - nd.com[1]);
-                    const float fz = (float)(pz - nd.com[2]);
-                    const float r2 = fx * fx + fy * fy + fz * fz;
-                    const float inv = rsqrtf(r2);
-                    const float inv2 = inv * inv;
-                    const float inv3 = inv * inv2;
-                    const float qxy = nd.q[0] * fx * fx + nd.q[1] * fy * fy + nd.q[2] * fz * fz +
-                                      2.f * (nd.q[3] * fx * fy + nd.q[4] * fx * fz + nd.q[5] * fy * fz);
-                    acc.add(-nd.mass * inv + 0.5f * nd.trq * inv3 - 1.5f * qxy * inv3 * inv2);
-                }
-            }
-            int s = 0, j = 0, j1 = 0;
-            if (nl > 0) {
-                const BhNode &nd = nodes[lq[lane]];
-                j = nd.lstart;
-                j1 = j + nd.lcount;
-            }
-            while (__any_sync(0xffffffffu, s < nl)) {
-                if (s < nl) {
-                    const float4 S = spos[j];
-                    // ost.c:186-191: float offsets of the two positions
-                    const float fx = P.x - S.x;
-                    const float fy = P.y - S.y;
-                    const float fz = P.z - S.z;
-                    const float r2 = fx * fx + fy * fy + fz * fz;
-                    if (r2 > 0.f) acc.add(-S.w * rsqrtf(r2));
-                    if (++j == j1 && ++s < nl) {
-                        const BhNode &nd = nodes[lq[s * 32 + lane]];
-                        j = nd.lstart;
-                        j1 = j + nd.lcount;
-                    }
-                }
-            }
-            nc = nl = 0;
-        };
-        while (true) {
-            const int i = (int)__reduce_min_sync(0xffffffffu, (unsigned)my);
-            if (i == INT_MAX) break;
-            if (my == i) {
-                const BhNode &nd = nodes[i];
-                const double dx = px - nd.com[0];
-                const double dy = py - nd.com[1];
-                const double dz = pz - nd.com[2];
-                // separately rounded, as the reference's treeopen (ost.c:79)
-                const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
-                                            __dmul_rn(dz, dz));
-                if (always_open || d2 < nd.open_r2) {
-                    if (nd.lcount > 0) lq[(nl++) * 32 + lane] = i;
-                    npp += nd.lcount;
-                    my = i + 1;
-                } else {
-                    cq[(nc++) * 32 + lane] = i;
-                    npc++;
-                    my = nd.skip;
-                }
-                if (my >= my_end) my = INT_MAX;
-            }
-            if (__any_sync(0xffffffffu, nc == kBhQueue || nl == kBhQueue)) flush();
-        }
-        flush();
-        if (valid) {
-            const int64_t o = tout ? tout[t] : t;
-            const float phi = acc.s + (-acc.c);
-            if (raw) raw[o] = phi;
-            if (out) {
-                double e = pp.potentfact != 0.0 ? (double)phi * pp.potentfact : (double)phi;
-                if (pp.add_bg && bg) e += bg[h];
-                out[o] = (float)e;  // penergy = potent*potentfact + halobgpotent
-            }
-        }
-    }
-    if (counters) {
-        for (int off = 16; off; off >>= 1) {
-            npp += __shfl_xor_sync(0xffffffffu, npp, off);
-            npc += __shfl_xor_sync(0xffffffffu, npc, off);
-        }
-        if (lane == 0) {
-            atomicAdd(counters + 0, npp);
-            atomicAdd(counters + 1, npc);
-        }
-    }
-}
-
-// The selected walk (GF_BH_ALGO): 0 the lockstep evaluation, 1 the queued one.
+// The walk over ntarget targets.  With GF_BH_DYN the grid is one resident
+// wave and each warp takes its next 32 targets from a counter in device
+// memory, so warps that drew cheap targets keep drawing and the launch ends
+// when the work does (with a static grid-stride split, the warps holding the
+// costliest targets finish last, alone).
 int launch_bh(gf_ctx *ctx, int64_t grid, int64_t ntarget, const float4 *tpos, const int32_t *thalo,
               const int32_t *tout, const float4 *spos, const int32_t *root, const int32_t *rend,
               const BhNode *nodes, const int32_t *direct, const double *bg, const PotentialParams &pp,
               float *out, float *raw, unsigned long long *counters) {
     const int block = GF_BH_BLOCK;
-    if (GF_BH_ALGO == 1) {
-        const size_t smem = (size_t)(block / 32) * 2 * kBhQueue * 32 * sizeof(int32_t);
-        GF_CUDA_TRY(cudaFuncSetAttribute(bh_list_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        bh_list_kernel<<<(int)grid, block, smem, ctx->stream>>>(ntarget, tpos, thalo, tout, spos, root, rend, nodes,
-                                                               direct, bg, pp, out, raw, counters);
-    } else {
-        bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, tout, spos, root, rend, nodes, direct,
-                                                        bg, pp, out, raw, counters);
+    unsigned long long *work = nullptr;
+    if (GF_BH_DYN) {
+        int per_sm = 0;
+        GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_kernel, block, 0));
+        grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)sm_count() * std::max(per_sm, 1)));
+        GF_TRY(ctx->work.reserve(256));
+        work = ctx->work.as<unsigned long long>();  // slot 0: this walk
+        GF_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long), ctx->stream));
     }
+    bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, tout, spos, root, rend, nodes, direct, bg,
+                                                    pp, out, raw, counters, work);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }

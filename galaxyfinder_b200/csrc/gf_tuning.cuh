@@ -37,8 +37,14 @@
 #ifndef GF_BH_BLOCK    // threads per block of bh_kernel
 #define GF_BH_BLOCK 128
 #endif
-#ifndef GF_BH_ALGO     // Barnes-Hut walk: 0 terms evaluated in the lockstep walk, 1 queued per lane
-#define GF_BH_ALGO 0
+#ifndef GF_BH_DYN      // Barnes-Hut walk: 1 = warps take targets from a work counter, 0 = grid-stride
+#define GF_BH_DYN 0
+#endif
+#ifndef GF_BH_ACC      // Barnes-Hut sums: 0 = FP32 with Kahan compensation, 1 = FP64
+#define GF_BH_ACC 0
+#endif
+#ifndef GF_KNNB_DYN    // float-key kNN: 1 = warps take buckets from a work counter, 0 = grid-stride
+#define GF_KNNB_DYN 0
 #endif
 #ifndef GF_BH_MINB
 #define GF_BH_MINB 1
@@ -68,7 +74,9 @@ static_assert(GF_KNNB_LANECERT == 0 || GF_KNNB_LANECERT == 1, "GF_KNNB_LANECERT"
 static_assert(GF_KNNB_QUEUE >= 0 && GF_KNNB_QUEUE <= 16, "GF_KNNB_QUEUE");
 static_assert(GF_KNNB_SEEDS >= 32 && GF_KNNB_SEEDS % 2 == 0, "GF_KNNB_SEEDS");
 static_assert(GF_BH_BLOCK % 32 == 0 && GF_BH_BLOCK <= 1024, "GF_BH_BLOCK");
-static_assert(GF_BH_ALGO == 0 || GF_BH_ALGO == 1, "GF_BH_ALGO");
+static_assert(GF_BH_DYN == 0 || GF_BH_DYN == 1, "GF_BH_DYN");
+static_assert(GF_KNNB_DYN == 0 || GF_KNNB_DYN == 1, "GF_KNNB_DYN");
+static_assert(GF_BH_ACC == 0 || GF_BH_ACC == 1, "GF_BH_ACC");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");
 static_assert(GF_FFT_PENCILS_64 >= 32 && GF_FFT_PENCILS_64 <= 128 &&
                   (GF_FFT_PENCILS_64 & (GF_FFT_PENCILS_64 - 1)) == 0, "GF_FFT_PENCILS_64");

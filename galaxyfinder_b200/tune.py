@@ -40,7 +40,7 @@ from . import build as B
 TUNE_DIR = B.PKG / "_tune"
 DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0, "GF_KNNB_LANECERT": 0,
             "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
-            "GF_BH_BLOCK": 128, "GF_BH_ALGO": 0,
+            "GF_BH_BLOCK": 128, "GF_BH_DYN": 0, "GF_BH_ACC": 0, "GF_KNNB_DYN": 0,
             "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TSC_TILE": 0, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
 
@@ -58,12 +58,14 @@ def stages(group: str):
                 [{"GF_KNN_ALGO": 1, "GF_KNNB_BLOCK": 32, "GF_KNNB_ARITY": 4}, {"GF_KNN_ALGO": 0}],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_SEEDS": n} for n in (32, 48, 64, 80, 96)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_LANECERT": c} for c in (0, 1)],
+                lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_DYN": d} for d in (0, 1)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_QUEUE": q} for q in (0, 2, 4, 8)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else
                 [{"GF_KNN_BLOCK": b, "GF_KNN_MINB": minb(b, r)} for b in (128, 256) for r in REGCAPS]]
     if group == "bh":
-        return [lambda base: [{"GF_BH_ALGO": a} for a in (0, 1)],
+        return [lambda base: [{"GF_BH_DYN": d} for d in (0, 1)],
+                lambda base: [{"GF_BH_ACC": a} for a in (0, 1)],
                 lambda base: [{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],
                 lambda base: [{"GF_BH_MINB": minb(base["GF_BH_BLOCK"], r)} for r in REGCAPS]]
     if group == "fft":

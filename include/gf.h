@@ -53,7 +53,7 @@ int gf_set_device(int device);
 uint64_t gf_kernel_launch_count(void);
 /* Compile-time launch parameter `name` of the loaded library (GF_KNN_ALGO,
  * GF_KNNB_BLOCK, GF_KNNB_ARITY, GF_KNNB_SEEDS, GF_KNNB_QUEUE, GF_KNNB_LANECERT,
- * GF_KNN_BLOCK, GF_KNN_MINB, GF_KNN_CHUNK, GF_BH_BLOCK, GF_BH_MINB, GF_BH_ALGO,
+ * GF_KNN_BLOCK, GF_KNN_MINB, GF_KNN_CHUNK, GF_BH_BLOCK, GF_BH_MINB, GF_BH_DYN, GF_BH_ACC, GF_KNNB_DYN,
  * GF_FFT_PENCILS, GF_FFT_PENCILS_64, GF_FFT_PENCILS_128, GF_TSC_TILE,
  * GF_TREE_BLOCK) in *value.
  * Returns GF_EINVAL for an unknown name. */

@@ -36,8 +36,9 @@ def test_search_space_is_valid():
             assert nonempty >= 1
         assert len(T.stages("knn")[1](base)) == (5 if algo == 2 else 0)  # seed windows
         assert len(T.stages("knn")[2](base)) == (2 if algo == 2 else 0)  # lane or warp certification
-        assert len(T.stages("knn")[3](base)) == (4 if algo == 2 else 0)  # survivor queues
-        assert len(T.stages("knn")[4](base)) == (3 if algo == 0 else 0)
+        assert len(T.stages("knn")[3](base)) == (2 if algo == 2 else 0)  # work counter or grid-stride
+        assert len(T.stages("knn")[4](base)) == (4 if algo == 2 else 0)  # survivor queues
+        assert len(T.stages("knn")[5](base)) == (3 if algo == 0 else 0)
 
 
 def test_tuned_params_become_flags(tmp_path, monkeypatch):
