@@ -53,7 +53,7 @@ struct Build {
     int32_t *first, *nchild, *lstart, *lcount;
     int32_t *sub, *pre;             // subtree size, preorder index
     int32_t *par;                   // BFS id of the parent, -1 for roots
-    int32_t *counter;               // [0] nodes allocated, [1] overflow flag
+    int32_t *counter;               // [0] nodes allocated, [1] overflow flag, [2] blocks done
     int32_t *lev;                   // level L holds BFS nodes [lev[L], lev[L+1])
 };
 
@@ -68,6 +68,7 @@ __global__ void init_build(int32_t nhalo, Build b) {
     if (threadIdx.x == 0) {
         b.counter[0] = nhalo;  // the roots are nodes 0 .. nhalo-1
         b.counter[1] = 0;
+        b.counter[2] = 0;
         b.lev[0] = 0;
         b.lev[1] = nhalo;
     }
@@ -307,11 +308,16 @@ __global__ void split_nodes(int L, int32_t ncap, int last, Build b) {
     b.first[node] = first;
     b.nchild[node] = nch;
     }
-}
-
-// The next level: the nodes allocated by split_nodes of level L.
-__global__ void close_level(int L, int32_t ncap, Build b) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) b.lev[L + 2] = min(b.counter[0], ncap);
+    // the last block to finish writes the next level's end: the nodes this
+    // level allocated (its children are numbered [lev[L+1], lev[L+2]))
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(b.counter + 2, 1) == (int)gridDim.x - 1) {
+            b.lev[L + 2] = min(atomicAdd(b.counter, 0), ncap);
+            b.counter[2] = 0;  // for the next level's launch
+        }
+    }
 }
 
 __global__ void scatter_particles(int64_t n, const float4 *__restrict__ pos_in,
@@ -566,8 +572,6 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
             scatter_particles<<<grid_n(n), kBlock, 0, s>>>(n, pos[cur], perm[cur], pnode[cur], pkey,
                                                            pos[cur ^ 1], perm[cur ^ 1],
                                                            pnode[cur ^ 1], b);
-            GF_LAUNCH_CHECK();
-            close_level<<<1, 32, 0, s>>>(L, (int32_t)ncap, b);
             GF_LAUNCH_CHECK();
             cur ^= 1;
             nlev = L + 1;
