@@ -412,7 +412,8 @@ struct StageGraph {
 namespace {
 
 std::vector<void *> context_buffers(gf_ctx *c) {
-    std::vector<void *> v = {c->hid.ptr, c->mesh.ptr, c->mesh_boxes.ptr, c->smooth_tables.ptr, c->particles.ptr};
+    std::vector<void *> v = {c->hid.ptr, c->mesh.ptr, c->mesh_boxes.ptr, c->smooth_tables.ptr, c->particles.ptr,
+                             c->work.ptr};
     for (auto &t : c->tmp) v.push_back(t.ptr);
     for (auto &t : c->tree) v.push_back(t.ptr);
     return v;
