@@ -99,13 +99,15 @@ struct KnnNode {
 
 // Node of the potential walk (preorder): monopole + quadrupole about the
 // centre of mass, opening radius^2 = dist2/theta2 (ost.c:72-83, 557-582).
-struct BhNode {
+// 80 bytes, 16-byte aligned: the walk reads it as five 16-byte loads.
+struct __align__(16) BhNode {
     double com[3];
     double open_r2;
     float mass, trq;
     float q[6];  // xx, yy, zz, xy, xz, yz second moments about the COM
     int32_t skip, lstart, lcount, count;
 };
+static_assert(sizeof(BhNode) == 80 && alignof(BhNode) == 16, "BhNode is read as five 16-byte words");
 
 struct TreeView {
     int32_t nhalo = 0, nnode = 0;
@@ -207,14 +209,33 @@ struct SmoothGroup {
     int64_t ntiles;
 };
 struct SmoothPlan {
-    std::vector<char> blob;  // [axes | tables | on-chip halos | per group: halos, starts]
-    size_t off_tab = 0, off_chip = 0;
-    int32_t nchip = 0;
+    // [axes | tables | on-chip halos | per group: halos, starts | zeroed-plane prefix]
+    std::vector<char> blob;
+    size_t off_tab = 0, off_chip = 0, off_zero = 0;
+    int32_t nchip = 0, nhalo = 0;
+    bool box_ok = false;  // every group an FFT axis: the box-restricted passes apply
     std::vector<SmoothGroup> groups;
 };
 int smooth_plan(int32_t nhalo, const gf_mesh_desc *mesh_host, const OnChipMeshes *onchip, SmoothPlan *plan);
 int smooth_launch(gf_ctx *ctx, const SmoothPlan &plan, const char *dbuf, const gf_mesh_desc *mesh_dev,
                   float *den, const OnChipMeshes *onchip = nullptr, const MeshBoxes *boxes = nullptr);
+// Copies the plan's blob into ctx->smooth_tables (through pinned staging);
+// *dbuf receives its device address.
+int smooth_upload(gf_ctx *ctx, const SmoothPlan &plan, char **dbuf);
+// The box-restricted mesh stage, for meshes that only findDen reads (the
+// stage): launch_mesh_boxes fills the occupied boxes from the particles
+// before any deposit; smooth_box_prepare counts the passes' tiles from the
+// boxes (into the uploaded blob at dbuf) and zeroes only each mesh's deposit
+// box (its evaluation box when nothing is deposited) — the rest of den is
+// never read; after the deposit, smooth_box_launch runs the three passes over
+// the boxes.  Needs plan.box_ok.
+int launch_mesh_boxes(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                      const int32_t *type, const int32_t *hid, int32_t nhalo, const gf_mesh_desc *mesh,
+                      int32_t *boxes);
+int smooth_box_prepare(gf_ctx *ctx, const SmoothPlan &plan, char *dbuf, const gf_mesh_desc *mesh_dev,
+                       float *den, const int32_t *boxes);
+int smooth_box_launch(gf_ctx *ctx, const SmoothPlan &plan, const char *dbuf, const gf_mesh_desc *mesh_dev,
+                      float *den, const int32_t *boxes, const OnChipMeshes *onchip = nullptr);
 
 // Single-mesh smoothing plan in one contiguous byte blob (see gf_smooth.cu):
 // [mesh desc | 3 axis tables | per axis: halo list, tile prefix | tables].

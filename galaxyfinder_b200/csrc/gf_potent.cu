@@ -68,6 +68,8 @@ __device__ double bg_potent_dev(double mvir, const PotentialParams &pp) {
     return vc2 * (1 - gc * log(1 + c));
 }
 
+// COUNT: interaction counters (bench and tests); off in the stage's walk.
+template <bool COUNT>
 __global__ void __launch_bounds__(GF_BH_BLOCK, GF_BH_MINB)
 bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__restrict__ thalo,
           const int32_t *__restrict__ tout, const float4 *__restrict__ spos,
@@ -106,16 +108,25 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
             const int i = (int)__reduce_min_sync(0xffffffffu, (unsigned)my);
             if (i == INT_MAX) break;
             if (my == i) {
-                const BhNode &nd = nodes[i];
-                const double dx = px - nd.com[0];
-                const double dy = py - nd.com[1];
-                const double dz = pz - nd.com[2];
+                // the node in 16-byte words: (com x, com y), (com z, open_r2),
+                // (mass, trq, qxx, qyy), (qzz, qxy, qxz, qyz), (skip, lstart, lcount, count)
+                // All five are loaded before the opening test (one broadcast
+                // line for the lanes at the node), so the moment loads of an
+                // accepted cell overlap the FP64 test instead of following it.
+                const double2 *nd2 = reinterpret_cast<const double2 *>(nodes + i);
+                const float4 *nf = reinterpret_cast<const float4 *>(nodes + i);
+                const double2 c01 = __ldg(nd2), c2r = __ldg(nd2 + 1);
+                const float4 mq = __ldg(nf + 2), q = __ldg(nf + 3);  // (mass, trq, q0, q1), (q2..q5)
+                const int4 links = __ldg(reinterpret_cast<const int4 *>(nodes + i) + 4);
+                const double dx = px - c01.x;
+                const double dy = py - c01.y;
+                const double dz = pz - c2r.x;
                 // separately rounded, as the reference's treeopen (ost.c:79)
                 const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
                                             __dmul_rn(dz, dz));
-                if (always_open || d2 < nd.open_r2) {
-                    const int l1 = nd.lstart + nd.lcount;
-                    for (int j = nd.lstart; j < l1; j++) {
+                if (always_open || d2 < c2r.y) {
+                    const int l1 = links.y + links.z;
+                    for (int j = links.y; j < l1; j++) {
                         const float4 S = spos[j];
                         // ost.c:186-191: float offsets of the two positions.  For
                         // float inputs the FP32 difference is the correctly
@@ -127,7 +138,7 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
                         const float r2 = fx * fx + fy * fy + fz * fz;
                         if (r2 > 0.f) acc.add(-S.w * rsqrtf(r2));
                     }
-                    npp += nd.lcount;
+                    if (COUNT) npp += links.z;
                     my = i + 1;
                 } else {
                     const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
@@ -135,11 +146,11 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
                     const float inv = rsqrtf(r2);
                     const float inv2 = inv * inv;
                     const float inv3 = inv * inv2;
-                    const float qxy = nd.q[0] * fx * fx + nd.q[1] * fy * fy + nd.q[2] * fz * fz +
-                                      2.f * (nd.q[3] * fx * fy + nd.q[4] * fx * fz + nd.q[5] * fy * fz);
-                    acc.add(-nd.mass * inv + 0.5f * nd.trq * inv3 - 1.5f * qxy * inv3 * inv2);
-                    npc++;
-                    my = nd.skip;
+                    const float qxy = mq.z * fx * fx + mq.w * fy * fy + q.x * fz * fz +
+                                      2.f * (q.y * fx * fy + q.z * fx * fz + q.w * fy * fz);
+                    acc.add(-mq.x * inv + 0.5f * mq.y * inv3 - 1.5f * qxy * inv3 * inv2);
+                    if (COUNT) npc++;
+                    my = links.x;
                 }
                 if (my >= my_end) my = INT_MAX;
             }
@@ -155,7 +166,7 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
             }
         }
     }
-    if (counters) {
+    if (COUNT && counters) {
         for (int off = 16; off; off >>= 1) {
             npp += __shfl_xor_sync(0xffffffffu, npp, off);
             npc += __shfl_xor_sync(0xffffffffu, npc, off);
@@ -167,8 +178,8 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
     }
 }
 
-// The walk over ntarget targets.  With GF_BH_DYN the grid is one resident
-// wave and each warp takes its next 32 targets from a counter in device
+// The walk over ntarget targets on a grid of one resident wave.  With
+// GF_BH_DYN each warp takes its next 32 targets from a counter in device
 // memory, so warps that drew cheap targets keep drawing and the launch ends
 // when the work does (with a static grid-stride split, the warps holding the
 // costliest targets finish last, alone).
@@ -178,16 +189,19 @@ int launch_bh(gf_ctx *ctx, int64_t grid, int64_t ntarget, const float4 *tpos, co
               float *out, float *raw, unsigned long long *counters) {
     const int block = GF_BH_BLOCK;
     unsigned long long *work = nullptr;
+    // a grid of 1.6 waves (16 blocks per SM requested, 10 resident) would
+    // leave 40 % of the SMs' block slots empty in its second wave
+    auto kern = counters ? bh_kernel<true> : bh_kernel<false>;
+    int per_sm = 0;
+    GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0));
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)sm_count() * std::max(per_sm, 1)));
     if (GF_BH_DYN) {
-        int per_sm = 0;
-        GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bh_kernel, block, 0));
-        grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)sm_count() * std::max(per_sm, 1)));
         GF_TRY(ctx->work.reserve(256));
         work = ctx->work.as<unsigned long long>();  // slot 0: this walk
         GF_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long), ctx->stream));
     }
-    bh_kernel<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, tout, spos, root, rend, nodes, direct, bg,
-                                                    pp, out, raw, counters, work);
+    kern<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, tout, spos, root, rend, nodes, direct, bg, pp,
+                                               out, raw, counters, work);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }

@@ -656,6 +656,233 @@ smooth_fft_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh
     }
 }
 
+// ------------------------------------------------- box-restricted passes
+// The stage's meshes are read only by findDen, at the cells of the
+// evaluation box E (the stencils of every particle); the deposit writes only
+// the deposit box D (E contains D).  Each pass then needs only part of the
+// mesh, and every cell it reads outside D is a known zero:
+//   x: rows (y, z) in D_y x D_z; reads x in D_x (zero elsewhere); writes x in E_x
+//   y: columns (x, z) in E_x x D_z; reads y in D_y; writes y in E_y
+//   z: columns (x, y) in E_x x E_y; reads z in D_z; writes z in E_z
+// so only D has to be zeroed before the deposit, and findDen reads exactly
+// the cells the z pass wrote.  The FFT of a pencil whose zeros come from
+// registers instead of memory is the same computation, so the values at the
+// cells findDen reads equal those of full passes over a zeroed mesh (up to
+// the pairing of real pencils into complex ones, a rounding-level change).
+// A mesh with no deposited particle gets its evaluation box zeroed instead
+// and no pass.  The tile lists are counted on the device from the boxes
+// (a CUDA graph replays them for new particle positions).
+struct BoxGeom {
+    int u0, nu, v0, nv;                // pencil grid: u fastest
+    int ustride, vstride, sstride;     // float offsets within the mesh
+    int l0, l1, s0, s1;                // read and write ranges along the pencil
+};
+
+__device__ __forceinline__ int box_len(int lo, int hi) { return hi >= lo ? hi - lo + 1 : 0; }
+
+template <int AXIS>
+__device__ __forceinline__ BoxGeom box_geom(const gf_mesh_desc &m, const int32_t *__restrict__ bx) {
+    const int mx = 2 * (m.nx / 2 + 1);
+    BoxGeom g;
+    if (AXIS == 0) {
+        g.u0 = bx[2]; g.nu = box_len(bx[2], bx[3]); g.v0 = bx[4]; g.nv = box_len(bx[4], bx[5]);
+        g.ustride = mx; g.vstride = mx * m.ny; g.sstride = 1;
+        g.l0 = bx[0]; g.l1 = bx[1]; g.s0 = bx[6]; g.s1 = bx[7];
+    } else if (AXIS == 1) {
+        g.u0 = bx[6]; g.nu = box_len(bx[6], bx[7]); g.v0 = bx[4]; g.nv = box_len(bx[4], bx[5]);
+        g.ustride = 1; g.vstride = mx * m.ny; g.sstride = mx;
+        g.l0 = bx[2]; g.l1 = bx[3]; g.s0 = bx[8]; g.s1 = bx[9];
+    } else {
+        g.u0 = bx[6]; g.nu = box_len(bx[6], bx[7]); g.v0 = bx[8]; g.nv = box_len(bx[8], bx[9]);
+        g.ustride = 1; g.vstride = mx; g.sstride = mx * m.ny;
+        g.l0 = bx[4]; g.l1 = bx[5]; g.s0 = bx[10]; g.s1 = bx[11];
+    }
+    if (bx[0] > bx[1]) g.nu = g.nv = 0;  // nothing deposited: no pass
+    return g;
+}
+
+__device__ __forceinline__ int64_t box_tiles(int axis, const int32_t *__restrict__ bx, int pmax) {
+    if (bx[0] > bx[1]) return 0;
+    int64_t pen;
+    if (axis == 0) pen = (int64_t)box_len(bx[2], bx[3]) * box_len(bx[4], bx[5]);
+    else if (axis == 1) pen = (int64_t)box_len(bx[6], bx[7]) * box_len(bx[4], bx[5]);
+    else pen = (int64_t)box_len(bx[6], bx[7]) * box_len(bx[8], bx[9]);
+    return (pen + pmax - 1) / pmax;
+}
+
+// z planes zeroed before the deposit: those of D, or of E when D is empty
+__device__ __forceinline__ int64_t box_zero_planes(const gf_mesh_desc &m, const int32_t *__restrict__ bx) {
+    if (m.ptype == kMeshOnChip) return 0;
+    return bx[0] <= bx[1] ? box_len(bx[4], bx[5]) : box_len(bx[10], bx[11]);
+}
+
+constexpr int kBoxMaxGroups = 16;
+struct BoxPlanGroup {
+    const int32_t *halos;
+    int64_t *starts;  // ngroup + 1, written here
+    int32_t ngroup, axis, pmax;
+};
+struct BoxPlanArgs {
+    int32_t ngroups, nhalo;
+    BoxPlanGroup g[kBoxMaxGroups];
+    const int32_t *boxes;
+    const gf_mesh_desc *mesh;
+    int64_t *zstart;  // nhalo + 1, written here
+};
+
+// Exclusive prefix sums of the per-halo tile counts of every group (block
+// g < ngroups) and of the zeroed planes of every mesh (block ngroups).
+__global__ void __launch_bounds__(1024) box_plan_kernel(BoxPlanArgs a) {
+    __shared__ int64_t part[1024];
+    const bool zero = (int)blockIdx.x == a.ngroups;
+    const BoxPlanGroup G = zero ? BoxPlanGroup{nullptr, a.zstart, a.nhalo, 0, 1} : a.g[blockIdx.x];
+    auto count = [&](int i) -> int64_t {
+        if (zero) return box_zero_planes(a.mesh[i], a.boxes + (int64_t)kMeshBoxInts * i);
+        return box_tiles(G.axis, a.boxes + (int64_t)kMeshBoxInts * G.halos[i], G.pmax);
+    };
+    const int cnt = G.ngroup, per = (cnt + 1023) / 1024;
+    const int i0 = min(cnt, (int)threadIdx.x * per), i1 = min(cnt, i0 + per);
+    int64_t s = 0;
+    for (int i = i0; i < i1; i++) s += count(i);
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // inclusive scan (Hillis-Steele)
+        const int64_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int64_t run = part[threadIdx.x] - s;
+    for (int i = i0; i < i1; i++) {
+        G.starts[i] = run;
+        run += count(i);
+    }
+    if (threadIdx.x == 1023) G.starts[cnt] = part[1023];
+}
+
+// Contiguous share [t0, t1) of `total` items for this block.
+__device__ __forceinline__ void block_share(int64_t total, int64_t &t0, int64_t &t1) {
+    const int64_t per = (total + gridDim.x - 1) / gridDim.x;
+    t0 = min(total, (int64_t)blockIdx.x * per);
+    t1 = min(total, t0 + per);
+}
+
+// The entry i of a prefix array with starts[i] <= b < starts[i + 1],
+// searching upwards from a known lower bound.
+__device__ __forceinline__ int prefix_find(const int64_t *__restrict__ starts, int lo, int hi, int64_t b) {
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(starts + mid) <= b) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) zero_box_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh,
+                                                       const int32_t *__restrict__ boxes,
+                                                       const int64_t *__restrict__ zstart, int32_t nhalo) {
+    int64_t t0, t1;
+    block_share(zstart[nhalo], t0, t1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int h = -1;
+    for (int64_t b = t0; b < t1; b++) {
+        h = (h < 0 || __ldg(zstart + h + 1) <= b) ? prefix_find(zstart, max(h, 0), nhalo, b) : h;
+        const gf_mesh_desc m = mesh[h];
+        const int32_t *bx = boxes + (int64_t)kMeshBoxInts * h;
+        const int o = bx[0] <= bx[1] ? 0 : 6;  // D, or E when nothing was deposited
+        const int z = bx[o + 4] + (int)(b - zstart[h]);
+        const int64_t mx = 2 * (m.nx / 2 + 1);
+        float *plane = den + m.off + mx * (int64_t)m.ny * z;
+        for (int y = bx[o + 2] + warp; y <= bx[o + 3]; y += 8)
+            for (int x = bx[o] + lane; x <= bx[o + 1]; x += 32) plane[x + mx * y] = 0.f;
+    }
+}
+
+template <int AXIS, int LOGN>
+__global__ void __launch_bounds__(FftTile<LOGN>::NT)
+smooth_box_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh, GroupLaunch g,
+                  const AxisTable *__restrict__ axes, const float *__restrict__ tables,
+                  const int32_t *__restrict__ boxes) {
+    constexpr int N = 1 << LOGN;
+    constexpr int P = FftTile<LOGN>::P;
+    constexpr int NT = FftTile<LOGN>::NT;
+    using L = FftLayout<N>;
+    extern __shared__ float2 smem[];
+    __shared__ int32_t pb[P];  // offset of each pencil of the tile within its mesh
+    float2 *b0 = smem;
+    float2 *b1 = smem + (P / 2) * L::SN;
+    float *fa = reinterpret_cast<float *>(b0);
+    int64_t t0, t1;
+    block_share(g.tile_start[g.ngroup], t0, t1);
+    int gi = -1;
+    for (int64_t tb = t0; tb < t1; tb++) {
+        gi = (gi < 0 || __ldg(g.tile_start + gi + 1) <= tb) ? prefix_find(g.tile_start, max(gi, 0), g.ngroup, tb)
+                                                           : gi;
+        const int h = g.halos[gi];
+        const gf_mesh_desc m = mesh[h];
+        const BoxGeom q = box_geom<AXIS>(m, boxes + (int64_t)kMeshBoxInts * h);
+        const int64_t f0 = (tb - g.tile_start[gi]) * P;
+        const int npen = (int)min((int64_t)P, (int64_t)q.nu * q.nv - f0);
+        if (threadIdx.x < P) {
+            const int64_t f = f0 + threadIdx.x;
+            const int v = (int)(f / q.nu), u = (int)(f - (int64_t)v * q.nu);
+            pb[threadIdx.x] = (q.u0 + u) * q.ustride + (q.v0 + v) * q.vstride;  // unused beyond npen
+        }
+        __syncthreads();
+        const float *gm = den + m.off;
+        const int npair = (npen + 1) >> 1;
+        if (AXIS == 0) {  // rows: consecutive threads walk along a row
+            constexpr int PER = P * N / NT;
+            float v[PER];
+#pragma unroll
+            for (int r = 0; r < PER; r++) {
+                const int e = threadIdx.x + r * NT;
+                const int p = e >> LOGN, s = e & (N - 1);
+                v[r] = (p < npen && s >= q.l0 && s <= q.l1) ? gm[pb[p] + s] : 0.f;
+            }
+#pragma unroll
+            for (int r = 0; r < PER; r++) {
+                const int e = threadIdx.x + r * NT;
+                const int p = e >> LOGN, s = e & (N - 1);
+                fa[2 * L::at(p >> 1, s) + (p & 1)] = v[r];
+            }
+        } else {  // columns: consecutive threads take consecutive pencils
+            constexpr int NG = NT / P;
+            constexpr int PER = N / NG;
+            const int p = threadIdx.x % P;
+            const int w = threadIdx.x / P;
+            float v[PER];
+#pragma unroll
+            for (int r = 0; r < PER; r++) {
+                const int s = w + r * NG;
+                v[r] = (p < npen && s >= q.l0 && s <= q.l1) ? gm[pb[p] + s * q.sstride] : 0.f;
+            }
+#pragma unroll
+            for (int r = 0; r < PER; r++) fa[2 * L::at(p >> 1, w + r * NG) + (p & 1)] = v[r];
+        }
+        __syncthreads();
+        const AxisTable at = axes[3 * h + AXIS];
+        const float2 *tw = reinterpret_cast<const float2 *>(tables + at.tab_off);
+        const float *filt = tables + at.tab_off + 2 * N;
+        fft_filter_ifft<LOGN>(b0, b1, npair, tw, filt);
+        const float *fs = reinterpret_cast<const float *>(b0);
+        float *gd = den + m.off;
+        if (AXIS == 0) {
+            for (int e = threadIdx.x; e < npen * N; e += NT) {
+                const int p = e >> LOGN, s = e & (N - 1);
+                if (s >= q.s0 && s <= q.s1) gd[pb[p] + s] = fs[2 * L::at(p >> 1, s) + (p & 1)];
+            }
+        } else {
+            constexpr int NG = NT / P;
+            const int p = threadIdx.x % P;
+            if (p < npen) {
+                for (int s = q.s0 + threadIdx.x / P; s <= q.s1; s += NG)
+                    gd[pb[p] + s * q.sstride] = fs[2 * L::at(p >> 1, s) + (p & 1)];
+            }
+        }
+        __syncthreads();  // the tile buffers and pb are reused by the next tile
+    }
+}
+
 int ilog2_exact(int n) {
     if (n <= 0 || (n & (n - 1))) return -1;
     int l = 0;
@@ -856,7 +1083,12 @@ int smooth_plan(int32_t nhalo, const gf_mesh_desc *mesh_host, const OnChipMeshes
             g.start.push_back(g.start.back() + c);
         }
     }
-    // one blob: [axes | tables | on-chip halos | per group: halos, starts]
+    // the box-restricted passes (smooth_box_launch) cover FFT axes only
+    plan->box_ok = groups.size() <= (size_t)kBoxMaxGroups;
+    for (const Group &g : groups)
+        if (path_of(g.n) != PATH_FFT8 || g.pmax != fft_tile_pencils(g.n)) plan->box_ok = false;
+    plan->nhalo = nhalo;
+    // one blob: [axes | tables | on-chip halos | per group: halos, starts | zeroed-plane prefix]
     auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
     size_t off = align(axes.size() * sizeof(AxisTable));
     plan->off_tab = off;
@@ -871,6 +1103,8 @@ int smooth_plan(int32_t nhalo, const gf_mesh_desc *mesh_host, const OnChipMeshes
         off_s[i] = off;
         off = align(off + groups[i].start.size() * sizeof(int64_t));
     }
+    plan->off_zero = off;
+    off = align(off + ((size_t)nhalo + 1) * sizeof(int64_t));
     plan->blob.assign(off, 0);
     char *hbuf = plan->blob.data();
     memcpy(hbuf, axes.data(), axes.size() * sizeof(AxisTable));
@@ -930,11 +1164,8 @@ int smooth_launch(gf_ctx *ctx, const SmoothPlan &plan, const char *dbuf, const g
     return GF_OK;
 }
 
-int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
-                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip,
-                  const MeshBoxes *boxes) {
-    SmoothPlan plan;
-    GF_TRY(smooth_plan(nhalo, mesh_host, onchip, &plan));
+int smooth_upload(gf_ctx *ctx, const SmoothPlan &plan, char **dbuf) {
+    *dbuf = nullptr;
     if (plan.blob.empty()) return GF_OK;
     const size_t total = plan.blob.size();
     GF_TRY(ctx->smooth_tables.reserve(total));
@@ -942,9 +1173,114 @@ int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
     // the pinned staging buffer may still feed an earlier asynchronous copy
     GF_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     memcpy(ctx->pin[3].ptr, plan.blob.data(), total);
-    char *dbuf = ctx->smooth_tables.as<char>();
-    GF_CUDA_TRY(cudaMemcpyAsync(dbuf, ctx->pin[3].ptr, total, cudaMemcpyHostToDevice, ctx->stream));
+    *dbuf = ctx->smooth_tables.as<char>();
+    GF_CUDA_TRY(cudaMemcpyAsync(*dbuf, ctx->pin[3].ptr, total, cudaMemcpyHostToDevice, ctx->stream));
+    return GF_OK;
+}
+
+int smooth_meshes(gf_ctx *ctx, int32_t nhalo, const gf_mesh_desc *mesh_host,
+                  const gf_mesh_desc *mesh_dev, float *den, const OnChipMeshes *onchip,
+                  const MeshBoxes *boxes) {
+    SmoothPlan plan;
+    GF_TRY(smooth_plan(nhalo, mesh_host, onchip, &plan));
+    if (plan.blob.empty()) return GF_OK;
+    char *dbuf = nullptr;
+    GF_TRY(smooth_upload(ctx, plan, &dbuf));
     return smooth_launch(ctx, plan, dbuf, mesh_dev, den, onchip, boxes);
+}
+
+namespace {
+
+template <int AXIS, int LOGN>
+int launch_box_fft(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunch g, int64_t max_tiles,
+                   const AxisTable *axes, const float *tables, const int32_t *boxes) {
+    constexpr int N = 1 << LOGN;
+    const int threads = FftTile<LOGN>::NT;
+    const size_t smem = (size_t)2 * (FftTile<LOGN>::P / 2) * FftLayout<N>::SN * sizeof(float2);
+    auto kern = smooth_box_kernel<AXIS, LOGN>;
+    GF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    GF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    // one resident wave; every block takes a contiguous share of the tiles
+    // the device counted (at most max_tiles, the whole-mesh count)
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(max_tiles, (int64_t)sm_count() * std::max(per_sm, 1)));
+    kern<<<(unsigned)grid, threads, smem, ctx->stream>>>(den, mesh_dev, g, axes, tables, boxes);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
+template <int AXIS>
+int launch_box_group(gf_ctx *ctx, float *den, const gf_mesh_desc *mesh_dev, GroupLaunch g, int64_t max_tiles,
+                     int n, const AxisTable *axes, const float *tables, const int32_t *boxes) {
+    if (max_tiles == 0) return GF_OK;
+    switch (ilog2_exact(n)) {
+        case 6: return launch_box_fft<AXIS, 6>(ctx, den, mesh_dev, g, max_tiles, axes, tables, boxes);
+        case 7: return launch_box_fft<AXIS, 7>(ctx, den, mesh_dev, g, max_tiles, axes, tables, boxes);
+        case 8: return launch_box_fft<AXIS, 8>(ctx, den, mesh_dev, g, max_tiles, axes, tables, boxes);
+        case 9: return launch_box_fft<AXIS, 9>(ctx, den, mesh_dev, g, max_tiles, axes, tables, boxes);
+        default: break;
+    }
+    set_status(GF_EINVAL, "box-restricted smoothing of a %d-cell axis (FFT axes of 64..512 cells only)", n);
+    return GF_EINVAL;
+}
+
+}  // namespace
+
+int smooth_box_prepare(gf_ctx *ctx, const SmoothPlan &plan, char *dbuf, const gf_mesh_desc *mesh_dev,
+                       float *den, const int32_t *boxes) {
+    if (plan.blob.empty() || plan.nhalo <= 0) return GF_OK;
+    if (!plan.box_ok) {
+        set_status(GF_EINVAL, "the box-restricted mesh passes need FFT axes of 64..512 cells");
+        return GF_EINVAL;
+    }
+    BoxPlanArgs a{};
+    a.ngroups = (int32_t)plan.groups.size();
+    a.nhalo = plan.nhalo;
+    for (size_t i = 0; i < plan.groups.size(); i++) {
+        const SmoothGroup &sg = plan.groups[i];
+        a.g[i].halos = reinterpret_cast<const int32_t *>(dbuf + sg.off_halos);
+        a.g[i].starts = reinterpret_cast<int64_t *>(dbuf + sg.off_starts);
+        a.g[i].ngroup = sg.ngroup;
+        a.g[i].axis = sg.axis;
+        a.g[i].pmax = sg.pmax;
+    }
+    a.boxes = boxes;
+    a.mesh = mesh_dev;
+    a.zstart = reinterpret_cast<int64_t *>(dbuf + plan.off_zero);
+    box_plan_kernel<<<a.ngroups + 1, 1024, 0, ctx->stream>>>(a);
+    GF_LAUNCH_CHECK();
+    zero_box_kernel<<<sm_count() * 8, 256, 0, ctx->stream>>>(den, mesh_dev, boxes, a.zstart, plan.nhalo);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
+
+int smooth_box_launch(gf_ctx *ctx, const SmoothPlan &plan, const char *dbuf, const gf_mesh_desc *mesh_dev,
+                      float *den, const int32_t *boxes, const OnChipMeshes *onchip) {
+    if (plan.blob.empty()) return GF_OK;
+    const AxisTable *d_axes = reinterpret_cast<const AxisTable *>(dbuf);
+    const float *d_tab = reinterpret_cast<const float *>(dbuf + plan.off_tab);
+    // axes in order x, y, z: each pass reads what the previous one wrote
+    for (int axis = 0; axis < 3; axis++) {
+        for (const SmoothGroup &g : plan.groups) {
+            if (g.axis != axis) continue;
+            GroupLaunch gl;
+            gl.halos = reinterpret_cast<const int32_t *>(dbuf + g.off_halos);
+            gl.tile_start = reinterpret_cast<const int64_t *>(dbuf + g.off_starts);
+            gl.ngroup = g.ngroup;
+            if (axis == 0) GF_TRY(launch_box_group<0>(ctx, den, mesh_dev, gl, g.ntiles, g.n, d_axes, d_tab, boxes));
+            else if (axis == 1) GF_TRY(launch_box_group<1>(ctx, den, mesh_dev, gl, g.ntiles, g.n, d_axes, d_tab, boxes));
+            else GF_TRY(launch_box_group<2>(ctx, den, mesh_dev, gl, g.ntiles, g.n, d_axes, d_tab, boxes));
+        }
+    }
+    if (plan.nchip) {
+        SmoothPlan chip_only;
+        chip_only.blob = {0};
+        chip_only.off_tab = plan.off_tab;
+        chip_only.off_chip = plan.off_chip;
+        chip_only.nchip = plan.nchip;
+        GF_TRY(smooth_launch(ctx, chip_only, dbuf, mesh_dev, den, onchip, nullptr));
+    }
+    return GF_OK;
 }
 
 }  // namespace gf

@@ -248,23 +248,13 @@ int stage_run_locked(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg,
     }
     tm.mark();  // 3
     // ---- 4. TSC mesh -> smoothing -> findDen
+    bool used_box_mode = false;
     if (cfg->do_mesh) {
         GF_TRY(ctx->tmp[3].reserve(sizeof(float) * (size_t)std::max<int64_t>(dev_cells, 1)));
         float *den = ctx->tmp[3].as<float>();
-        GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * dev_cells, s));
         const double vf = tsc_volfact();
-        // batch order: the deposit's float sums in octree order were faster
-        // (2.73 -> 2.34 ms) but put the densest cells of the 5e7-particle
-        // cluster 1.04e-5 from an FP64 deposit, past the 1e-5 target
-        // the occupied boxes let the smoothing skip all-zero pencils, and its
-        // last pass the columns no particle's findDen stencil reads
         GF_TRY(ctx->mesh_boxes.reserve(sizeof(int32_t) * kMeshBoxInts * (size_t)std::max(nh, 1)));
         int32_t *boxes = ctx->mesh_boxes.as<int32_t>();
-        GF_TRY(launch_stage_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, b->pstart,
-                                    need_tree ? ctx->last_tree.perm : nullptr,
-                                    need_tree ? ctx->last_tree.phalo : nullptr, nh, mesh_dev, den, vf, boxes));
-        if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, dev_cells, vf));
-        tm.mark();  // 4
         OnChipMeshes oc;
         if (!onchip_halos.empty()) {
             if (!o->dens_mesh || !volfact_folds(vf)) {
@@ -283,10 +273,40 @@ int stage_run_locked(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg,
             oc.volfold = (float)vf;
             oc.densph = o->dens_mesh;
         }
-        MeshBoxes mb;
-        mb.dev = boxes;
-        mb.trim_last = true;  // den is read only by find_den below
-        GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den, &oc, &mb));
+        SmoothPlan sp;
+        GF_TRY(smooth_plan(nh, mesh.data(), onchip_halos.empty() ? nullptr : &oc, &sp));
+        // only findDen reads the stage's meshes: with FFT axes and a folding
+        // volfact the passes run over the occupied boxes, and only the deposit
+        // boxes are zeroed (the rest of den is never read)
+        const bool box_mode = sp.box_ok && volfact_folds(vf) && !sp.blob.empty();
+        used_box_mode = box_mode;
+        char *dbuf = nullptr;
+        if (box_mode) {
+            GF_TRY(smooth_upload(ctx, sp, &dbuf));
+            GF_TRY(launch_mesh_boxes(ctx, n, xr, yr, zr, b->type, hid, nh, mesh_dev, boxes));
+            GF_TRY(smooth_box_prepare(ctx, sp, dbuf, mesh_dev, den, boxes));
+        } else {
+            GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * dev_cells, s));
+        }
+        // batch order: the deposit's float sums in octree order were faster
+        // (2.73 -> 2.34 ms) but put the densest cells of the 5e7-particle
+        // cluster 1.04e-5 from an FP64 deposit, past the 1e-5 target
+        // the occupied boxes let the smoothing skip all-zero pencils, and its
+        // last pass the columns no particle's findDen stencil reads
+        GF_TRY(launch_stage_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, b->pstart,
+                                    need_tree ? ctx->last_tree.perm : nullptr,
+                                    need_tree ? ctx->last_tree.phalo : nullptr, nh, mesh_dev, den, vf,
+                                    box_mode ? nullptr : boxes));
+        if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, dev_cells, vf));
+        tm.mark();  // 4
+        if (box_mode) {
+            GF_TRY(smooth_box_launch(ctx, sp, dbuf, mesh_dev, den, boxes, &oc));
+        } else {
+            MeshBoxes mb;
+            mb.dev = boxes;
+            mb.trim_last = true;  // den is read only by find_den below
+            GF_TRY(smooth_meshes(ctx, nh, mesh.data(), mesh_dev, den, &oc, &mb));
+        }
         tm.mark();  // 5
         if (o->dens_mesh)
             GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh,
@@ -330,7 +350,12 @@ int stage_run_locked(gf_ctx *ctx, const gf_batch *b, const gf_stage_config *cfg,
                 if (m.ptype == kMeshOnChip) continue;
                 const int32_t *q = &bx[(size_t)kMeshBoxInts * h];
                 st->mesh_pass_cells += (int64_t)m.nx * len(q[2], q[3]) * len(q[4], q[5]);  // x pass
-                st->mesh_pass_cells += (int64_t)m.ny * m.nx * len(q[4], q[5]);              // y pass
+                if (used_box_mode) {  // y pass over the evaluation box's x only
+                    if (q[0] > q[1]) continue;  // nothing deposited: no pass
+                    st->mesh_pass_cells += (int64_t)m.ny * len(q[6], q[7]) * len(q[4], q[5]);
+                } else {
+                    st->mesh_pass_cells += (int64_t)m.ny * m.nx * len(q[4], q[5]);
+                }
                 st->mesh_pass_cells += (int64_t)m.nz * len(q[6], q[7]) * len(q[8], q[9]);  // z pass, trimmed
             }
         }
@@ -455,18 +480,31 @@ int stage_pass_graph(StageGraph &g) {
         const int64_t dev_cells = g.plan.dev_cells;
         GF_TRY(ctx->tmp[3].reserve(sizeof(float) * (size_t)std::max<int64_t>(dev_cells, 1)));
         float *den = ctx->tmp[3].as<float>();
-        GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * dev_cells, s));
         const double vf = tsc_volfact();
         GF_TRY(ctx->mesh_boxes.reserve(sizeof(int32_t) * kMeshBoxInts * (size_t)std::max(nh, 1)));
         int32_t *boxes = ctx->mesh_boxes.as<int32_t>();
+        // as the eager stage: passes over the occupied boxes, only the deposit
+        // boxes zeroed; the tile counts are recounted on the device each replay
+        const bool box_mode = g.smooth.box_ok && volfact_folds(vf) && !g.smooth.blob.empty();
+        if (box_mode) {
+            GF_TRY(launch_mesh_boxes(ctx, n, xr, yr, zr, b->type, hid, nh, mesh_dev, boxes));
+            GF_TRY(smooth_box_prepare(ctx, g.smooth, g.smooth_blob.as<char>(), mesh_dev, den, boxes));
+        } else {
+            GF_CUDA_TRY(cudaMemsetAsync(den, 0, sizeof(float) * dev_cells, s));
+        }
         GF_TRY(launch_stage_deposit(ctx, n, xr, yr, zr, b->mass, b->type, hid, b->pstart,
                                     g.plan.need_tree ? ctx->last_tree.perm : nullptr,
-                                    g.plan.need_tree ? ctx->last_tree.phalo : nullptr, nh, mesh_dev, den, vf, boxes));
+                                    g.plan.need_tree ? ctx->last_tree.phalo : nullptr, nh, mesh_dev, den, vf,
+                                    box_mode ? nullptr : boxes));
         if (!volfact_folds(vf)) GF_TRY(launch_scale(ctx, den, dev_cells, vf));
-        MeshBoxes mb;
-        mb.dev = boxes;
-        mb.trim_last = true;  // den is read only by find_den below
-        GF_TRY(smooth_launch(ctx, g.smooth, g.smooth_blob.as<char>(), mesh_dev, den, nullptr, &mb));
+        if (box_mode) {
+            GF_TRY(smooth_box_launch(ctx, g.smooth, g.smooth_blob.as<char>(), mesh_dev, den, boxes));
+        } else {
+            MeshBoxes mb;
+            mb.dev = boxes;
+            mb.trim_last = true;  // den is read only by find_den below
+            GF_TRY(smooth_launch(ctx, g.smooth, g.smooth_blob.as<char>(), mesh_dev, den, nullptr, &mb));
+        }
         if (o->dens_mesh)
             GF_TRY(launch_find_den(ctx, n, xr, yr, zr, hid, mesh_dev, den, o->dens_mesh,
                                    g.plan.need_tree ? ctx->last_tree.perm : nullptr));

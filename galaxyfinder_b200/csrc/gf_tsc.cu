@@ -106,6 +106,40 @@ __global__ void tsc_deposit_kernel(int64_t n, const double *__restrict__ x,
     }
 }
 
+// The occupied boxes alone, before any deposit: the stencil ranges of the
+// deposited particles (deposit box) and of every particle (evaluation box) of
+// each device-memory mesh, with the same stencils as the deposit.  The
+// box-restricted mesh stage zeroes only the deposit boxes from them.
+__global__ void mesh_box_kernel(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
+                                const double *__restrict__ z, const int32_t *__restrict__ type,
+                                const int32_t *__restrict__ hid, const gf_mesh_desc *__restrict__ mesh,
+                                int32_t *__restrict__ boxes) {
+    // whole warps step together (the box update reduces over the warp)
+    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x; t0 < n; t0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = t0 + threadIdx.x;
+        int hb = -1;
+        bool dep = false;
+        int c[6] = {0, 0, 0, 0, 0, 0};
+        if (p < n) {
+            const int h = hid ? hid[p] : 0;
+            const gf_mesh_desc m = mesh[h];
+            if (m.ptype != kMeshOnChip) {
+                TscStencil s;
+                float xd1, yd1, zd1;
+                tsc_cells(x[p], y[p], z[p], m, s, xd1, yd1, zd1);
+                if (tsc_in_mesh(s, m)) {  // particles outside are flagged by the deposit and findDen
+                    hb = h;
+                    dep = m.ptype == GF_TYPE_ALL || (type ? type[p] : GF_TYPE_DM) == m.ptype;
+                    c[0] = (int)s.i[0] - 1; c[1] = (int)s.i[0] + 1;
+                    c[2] = (int)s.j[0] - 1; c[3] = (int)s.j[0] + 1;
+                    c[4] = (int)s.k[0] - 1; c[5] = (int)s.k[0] + 1;
+                }
+            }
+        }
+        box_update(boxes, hb, dep, c);
+    }
+}
+
 // ---------------------------------------------------------------- tiled deposit
 // The deposit through shared-memory tiles.  A block takes kTileChunk
 // consecutive particles in octree order (spatial neighbours; the halos'
@@ -377,6 +411,18 @@ int launch_find_den(gf_ctx *ctx, int64_t n, const double *x, const double *y, co
 }
 
 bool volfact_folds(double v) { return is_pow2_double(v); }
+
+int launch_mesh_boxes(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
+                      const int32_t *type, const int32_t *hid, int32_t nhalo, const gf_mesh_desc *mesh,
+                      int32_t *boxes) {
+    const int64_t nint = (int64_t)kMeshBoxInts * std::max(nhalo, 1);
+    box_init_kernel<<<grid_for(nint, 256), 256, 0, ctx->stream>>>(boxes, nint);
+    GF_LAUNCH_CHECK();
+    if (n <= 0) return GF_OK;
+    mesh_box_kernel<<<grid_for(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, type, hid, mesh, boxes);
+    GF_LAUNCH_CHECK();
+    return GF_OK;
+}
 
 int launch_stage_deposit(gf_ctx *ctx, int64_t n, const double *x, const double *y, const double *z,
                          const double *mass, const int32_t *type, const int32_t *hid, const int64_t *pstart,
