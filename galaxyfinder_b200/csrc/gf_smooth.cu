@@ -710,10 +710,11 @@ __device__ __forceinline__ int64_t box_tiles(int axis, const int32_t *__restrict
     return (pen + pmax - 1) / pmax;
 }
 
-// z planes zeroed before the deposit: those of D, or of E when D is empty
-__device__ __forceinline__ int64_t box_zero_planes(const gf_mesh_desc &m, const int32_t *__restrict__ bx) {
+// rows (y, z) zeroed before the deposit: those of D, or of E when D is empty
+__device__ __forceinline__ int64_t box_zero_rows(const gf_mesh_desc &m, const int32_t *__restrict__ bx) {
     if (m.ptype == kMeshOnChip) return 0;
-    return bx[0] <= bx[1] ? box_len(bx[4], bx[5]) : box_len(bx[10], bx[11]);
+    const int o = bx[0] <= bx[1] ? 0 : 6;
+    return (int64_t)box_len(bx[o + 2], bx[o + 3]) * box_len(bx[o + 4], bx[o + 5]);
 }
 
 constexpr int kBoxMaxGroups = 16;
@@ -727,17 +728,17 @@ struct BoxPlanArgs {
     BoxPlanGroup g[kBoxMaxGroups];
     const int32_t *boxes;
     const gf_mesh_desc *mesh;
-    int64_t *zstart;  // nhalo + 1, written here
+    int64_t *zstart;  // nhalo + 1, written here: prefix of the rows to zero
 };
 
 // Exclusive prefix sums of the per-halo tile counts of every group (block
-// g < ngroups) and of the zeroed planes of every mesh (block ngroups).
+// g < ngroups) and of the zeroed rows of every mesh (block ngroups).
 __global__ void __launch_bounds__(1024) box_plan_kernel(BoxPlanArgs a) {
     __shared__ int64_t part[1024];
     const bool zero = (int)blockIdx.x == a.ngroups;
     const BoxPlanGroup G = zero ? BoxPlanGroup{nullptr, a.zstart, a.nhalo, 0, 1} : a.g[blockIdx.x];
     auto count = [&](int i) -> int64_t {
-        if (zero) return box_zero_planes(a.mesh[i], a.boxes + (int64_t)kMeshBoxInts * i);
+        if (zero) return box_zero_rows(a.mesh[i], a.boxes + (int64_t)kMeshBoxInts * i);
         return box_tiles(G.axis, a.boxes + (int64_t)kMeshBoxInts * G.halos[i], G.pmax);
     };
     const int cnt = G.ngroup, per = (cnt + 1023) / 1024;
@@ -777,23 +778,39 @@ __device__ __forceinline__ int prefix_find(const int64_t *__restrict__ starts, i
     return lo;
 }
 
+// Zeroes the rows of every mesh's deposit box (its evaluation box when
+// nothing is deposited): each warp takes a contiguous share of all rows
+// (balanced whatever the mesh sizes), its lanes store along x.
 __global__ void __launch_bounds__(256) zero_box_kernel(float *__restrict__ den, const gf_mesh_desc *__restrict__ mesh,
                                                        const int32_t *__restrict__ boxes,
                                                        const int64_t *__restrict__ zstart, int32_t nhalo) {
-    int64_t t0, t1;
-    block_share(zstart[nhalo], t0, t1);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int h = -1;
-    for (int64_t b = t0; b < t1; b++) {
-        h = (h < 0 || __ldg(zstart + h + 1) <= b) ? prefix_find(zstart, max(h, 0), nhalo, b) : h;
+    const int64_t total = zstart[nhalo];
+    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t per = (total + nw - 1) / nw;
+    int64_t r = min(total, w * per);
+    const int64_t r1 = min(total, r + per);
+    int h = 0;
+    while (r < r1) {
+        h = prefix_find(zstart, h, nhalo, r);
         const gf_mesh_desc m = mesh[h];
         const int32_t *bx = boxes + (int64_t)kMeshBoxInts * h;
         const int o = bx[0] <= bx[1] ? 0 : 6;  // D, or E when nothing was deposited
-        const int z = bx[o + 4] + (int)(b - zstart[h]);
+        const int nyb = box_len(bx[o + 2], bx[o + 3]);
+        const int64_t local = r - zstart[h];
+        int z = bx[o + 4] + (int)(local / nyb);
+        int y = bx[o + 2] + (int)(local % nyb);
         const int64_t mx = 2 * (m.nx / 2 + 1);
-        float *plane = den + m.off + mx * (int64_t)m.ny * z;
-        for (int y = bx[o + 2] + warp; y <= bx[o + 3]; y += 8)
-            for (int x = bx[o] + lane; x <= bx[o + 1]; x += 32) plane[x + mx * y] = 0.f;
+        const int64_t rend = min(r1, zstart[h + 1]);
+        for (; r < rend; r++) {
+            float *row = den + m.off + mx * (y + (int64_t)m.ny * z);
+            for (int x = bx[o] + lane; x <= bx[o + 1]; x += 32) row[x] = 0.f;
+            if (++y > bx[o + 3]) {
+                y = bx[o + 2];
+                z++;
+            }
+        }
     }
 }
 
