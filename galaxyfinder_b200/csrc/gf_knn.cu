@@ -749,7 +749,11 @@ knn_bucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32_
 // exact distances in that order and insertion-sorts only where near-ties
 // reversed the float order) or by the warp one query at a time with a
 // bitonic sort of the exact keys.
-constexpr int kFBucketWarpBytes = 32 * 32 * 8 + 32 * (int)sizeof(KnnNode) + 32 * 16 + 32 * 4 +
+// Nodes of the walk staged per warp in shared memory (GF_KNNB_WIN at a time;
+// 0: every node is read from global memory through L1).  A smaller window
+// leaves room for more resident warps.
+constexpr int kWin = GF_KNNB_WIN;
+constexpr int kFBucketWarpBytes = 32 * 32 * 8 + kWin * (int)sizeof(KnnNode) + 32 * 16 + 32 * 4 +
                                   32 * GF_KNNB_QUEUE * 8;
 
 __device__ __forceinline__ uint64_t pack_key(float f, int id) {
@@ -790,7 +794,7 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
     unsigned char *ws = smem + (size_t)(threadIdx.x >> 5) * kFBucketWarpBytes;
     uint64_t *KH = reinterpret_cast<uint64_t *>(ws);
     KnnNode *win = reinterpret_cast<KnnNode *>(ws + 32 * 32 * 8);
-    float4 *cpos = reinterpret_cast<float4 *>(ws + 32 * 32 * 8 + 32 * sizeof(KnnNode));
+    float4 *cpos = reinterpret_cast<float4 *>(ws + 32 * 32 * 8 + kWin * sizeof(KnnNode));
     int *cid = reinterpret_cast<int *>(cpos + 32);
     int *win_w = reinterpret_cast<int *>(win);
     const int *nodes_w = reinterpret_cast<const int *>(nodes);
@@ -894,15 +898,20 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                         i = x1;
                         continue;
                     }
-                    if (i >= wb + 32 || i < wb) {
-                        wb = i;
-                        const int nw = min(32, w1 - wb) * 12;
-                        __syncwarp();
-                        for (int t = lane; t < nw; t += 32) win_w[t] = nodes_w[(int64_t)wb * 12 + t];
-                        __syncwarp();
+                    const float4 *nv;
+                    if (kWin > 0) {
+                        if (i >= wb + kWin || i < wb) {
+                            wb = i;
+                            const int nw = min(kWin, w1 - wb) * 12;
+                            __syncwarp();
+                            for (int t = lane; t < nw; t += 32) win_w[t] = nodes_w[(int64_t)wb * 12 + t];
+                            __syncwarp();
+                        }
+                        nv = reinterpret_cast<const float4 *>(win + (i - wb));
+                    } else {
+                        nv = reinterpret_cast<const float4 *>(nodes + i);  // one broadcast line
                     }
-                    const float4 *nv = reinterpret_cast<const float4 *>(win + (i - wb));
-                    const float4 n0 = nv[0], n1 = nv[1];
+                    const float4 n0 = kWin > 0 ? nv[0] : __ldg(nv), n1 = kWin > 0 ? nv[1] : __ldg(nv + 1);
                     const float gx = fmaxf(fmaxf(n0.x - Q.x, Q.x - n0.w), 0.f);
                     const float gy = fmaxf(fmaxf(n0.y - Q.y, Q.y - n1.x), 0.f);
                     const float gz = fmaxf(fmaxf(n0.z - Q.z, Q.z - n1.y), 0.f);
@@ -914,7 +923,7 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                         continue;
                     }
                     const int l0 = __float_as_int(n1.w);
-                    const int l1 = l0 + __float_as_int(nv[2].x);
+                    const int l1 = l0 + __float_as_int(kWin > 0 ? nv[2].x : __ldg(reinterpret_cast<const float *>(nv + 2)));
                     for (int base = l0; base < l1; base += 32) {
                         const int j = base + lane;
                         __syncwarp();

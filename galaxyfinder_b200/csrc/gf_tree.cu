@@ -108,6 +108,46 @@ __device__ __forceinline__ T group_sum(unsigned mask, T v) {
     return acc;
 }
 
+// Runs of a warp: lanes with equal node ids are consecutive (a node's active
+// particles are contiguous at every level), so a node's lanes form one run.
+// Inclusive segmented scans over the runs (five shuffle steps whatever the
+// run lengths); each run's last lane holds its reduction.
+struct WarpRuns {
+    int start;  // first lane of this lane's run
+    bool tail;  // last lane of its run
+};
+__device__ __forceinline__ WarpRuns warp_runs(int node) {
+    const int lane = threadIdx.x & 31;
+    const int prev = __shfl_up_sync(0xffffffffu, node, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != node);
+    WarpRuns r;
+    r.start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+    r.tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    return r;
+}
+template <class T, class Op>
+__device__ __forceinline__ T run_scan(T v, const WarpRuns &r, Op op) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const T u = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane - off >= r.start) v = op(v, u);
+    }
+    return v;
+}
+struct AddOp {
+    template <class T> __device__ __forceinline__ T operator()(T a, T b) const { return a + b; }
+};
+struct MinOp {
+    template <class T> __device__ __forceinline__ T operator()(T a, T b) const { return min(a, b); }
+};
+struct MaxOp {
+    template <class T> __device__ __forceinline__ T operator()(T a, T b) const { return max(a, b); }
+};
+struct FMaxOp {
+    __device__ __forceinline__ float operator()(float a, float b) const { return fmaxf(a, b); }
+};
+
 // Pass 1: mass and mass-weighted position per node (FP64 accumulation).
 __global__ void __launch_bounds__(kBlock)
 accum_mass(int64_t n, const float4 *__restrict__ pos, const int32_t *__restrict__ pnode, Build b) {
@@ -144,19 +184,35 @@ accum_mass(int64_t n, const float4 *__restrict__ pos, const int32_t *__restrict_
                 double *dst = threadIdx.x == 0 ? b.m : threadIdx.x == 1 ? b.mx : threadIdx.x == 2 ? b.my : b.mz;
                 atomicAdd(dst + s_node, a);
             }
-        } else {
-            const unsigned grp = __match_any_sync(0xffffffffu, node);
-            // settled particles (node < 0) have nothing to add; their group
-            // skips the sums (the other groups shuffle within their own masks)
+        } else if (__all_sync(0xffffffffu, node == __shfl_sync(0xffffffffu, node, 0))) {
+            // one node for the whole warp (settled warps add nothing)
             if (node >= 0) {
-                const double gw = group_sum(grp, w), gx = group_sum(grp, wx);
-                const double gy = group_sum(grp, wy), gz = group_sum(grp, wz);
-                if (lane == __ffs(grp) - 1) {
-                    atomicAdd(b.m + node, gw);
-                    atomicAdd(b.mx + node, gx);
-                    atomicAdd(b.my + node, gy);
-                    atomicAdd(b.mz + node, gz);
+                for (int off = 16; off; off >>= 1) {
+                    w += __shfl_xor_sync(0xffffffffu, w, off);
+                    wx += __shfl_xor_sync(0xffffffffu, wx, off);
+                    wy += __shfl_xor_sync(0xffffffffu, wy, off);
+                    wz += __shfl_xor_sync(0xffffffffu, wz, off);
                 }
+                if (lane == 0) {
+                    atomicAdd(b.m + node, w);
+                    atomicAdd(b.mx + node, wx);
+                    atomicAdd(b.my + node, wy);
+                    atomicAdd(b.mz + node, wz);
+                }
+            }
+        } else {
+            // several nodes: segmented sums over the warp's runs, added by
+            // each run's last lane (settled runs, node < 0, add nothing)
+            const WarpRuns r = warp_runs(node);
+            w = run_scan(w, r, AddOp());
+            wx = run_scan(wx, r, AddOp());
+            wy = run_scan(wy, r, AddOp());
+            wz = run_scan(wz, r, AddOp());
+            if (r.tail && node >= 0) {
+                atomicAdd(b.m + node, w);
+                atomicAdd(b.mx + node, wx);
+                atomicAdd(b.my + node, wy);
+                atomicAdd(b.mz + node, wz);
             }
         }
         __syncthreads();
@@ -175,14 +231,23 @@ __global__ void finalize_com(int L, Build b) {
 }
 
 // Pass 2: extents, max |x - com|^2, second moments and octant counts.
+// The 13 reductions (max r2, six moment sums, min and max of the three
+// coordinate keys) run over the block when all its particles share a node
+// (one atomic per value and block: the top levels of large halos), over the
+// warp when it does, else over the warp's runs.
 __global__ void __launch_bounds__(kBlock)
 accum_moments(int64_t n, const float4 *__restrict__ pos, const int32_t *__restrict__ pnode,
               uint8_t *__restrict__ pkey, int q5_asbuilt, Build b) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p - lane < n;
-         p += (int64_t)gridDim.x * blockDim.x) {
+    constexpr int kWarps = kBlock / 32;
+    __shared__ float s_f[7][kWarps];
+    __shared__ unsigned s_k[6][kWarps];
+    __shared__ int s_oct[8];
+    __shared__ int s_node;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < 8) s_oct[threadIdx.x] = 0;
+    for (int64_t base = blockIdx.x * (int64_t)kBlock; base < n; base += (int64_t)gridDim.x * kBlock) {
+        const int64_t p = base + threadIdx.x;
         const int node = p < n ? pnode[p] : -1;
-        if (__all_sync(0xffffffffu, node < 0)) continue;  // a warp of settled particles
         float v[7] = {0, 0, 0, 0, 0, 0, 0};  // max |x - com|^2, then q0..q5
         unsigned bx[6] = {~0u, ~0u, ~0u, 0u, 0u, 0u};
         int key = 0;
@@ -208,48 +273,75 @@ accum_moments(int64_t n, const float4 *__restrict__ pos, const int32_t *__restri
             key = ((double)P.x > cx ? 1 : 0) | ((double)P.y > cy ? 2 : 0) | ((double)P.z > cz ? 4 : 0);
             pkey[p] = (uint8_t)key;
         }
-        const unsigned grp = __match_any_sync(0xffffffffu, node);
-        const int leader = __ffs(grp) - 1;
-        float acc_r2 = v[0];
-        float acc_q[6] = {v[1], v[2], v[3], v[4], v[5], v[6]};
-        unsigned mn[3] = {bx[0], bx[1], bx[2]}, mxk[3] = {bx[3], bx[4], bx[5]};
-        if (grp == 0xffffffffu) {  // whole warp in one node: butterfly reduction
-            for (int off = 16; off; off >>= 1) {
-                acc_r2 = fmaxf(acc_r2, __shfl_xor_sync(0xffffffffu, acc_r2, off));
-                for (int i = 0; i < 6; i++) acc_q[i] += __shfl_xor_sync(0xffffffffu, acc_q[i], off);
+        if (threadIdx.x == 0) s_node = node;
+        __syncthreads();
+        const bool block_uniform = __syncthreads_and(node == s_node) && s_node >= 0;
+        const bool warp_uniform = __all_sync(0xffffffffu, node == __shfl_sync(0xffffffffu, node, 0));
+        if (block_uniform || warp_uniform) {  // butterfly over the warp (none for a settled warp)
+            for (int off = 16; node >= 0 && off; off >>= 1) {
+                v[0] = fmaxf(v[0], __shfl_xor_sync(0xffffffffu, v[0], off));
+                for (int i = 1; i < 7; i++) v[i] += __shfl_xor_sync(0xffffffffu, v[i], off);
                 for (int i = 0; i < 3; i++) {
-                    mn[i] = min(mn[i], __shfl_xor_sync(0xffffffffu, mn[i], off));
-                    mxk[i] = max(mxk[i], __shfl_xor_sync(0xffffffffu, mxk[i], off));
+                    bx[i] = min(bx[i], __shfl_xor_sync(0xffffffffu, bx[i], off));
+                    bx[3 + i] = max(bx[3 + i], __shfl_xor_sync(0xffffffffu, bx[3 + i], off));
                 }
             }
-        } else {  // lanes of several nodes: each group gathers its members
-            const float r2_self = acc_r2;
-            const float q_self[6] = {acc_q[0], acc_q[1], acc_q[2], acc_q[3], acc_q[4], acc_q[5]};
-            const unsigned mn_self[3] = {mn[0], mn[1], mn[2]}, mx_self[3] = {mxk[0], mxk[1], mxk[2]};
-            acc_r2 = 0.f;
-            for (int i = 0; i < 6; i++) acc_q[i] = 0.f;
-            for (int i = 0; i < 3; i++) { mn[i] = ~0u; mxk[i] = 0u; }
-            for (unsigned m = node >= 0 ? grp : 0u; m; m &= m - 1) {  // settled lanes: nothing to gather
-                const int src = __ffs(m) - 1;
-                acc_r2 = fmaxf(acc_r2, __shfl_sync(grp, r2_self, src));
-                for (int i = 0; i < 6; i++) acc_q[i] += __shfl_sync(grp, q_self[i], src);
-                for (int i = 0; i < 3; i++) {
-                    mn[i] = min(mn[i], __shfl_sync(grp, mn_self[i], src));
-                    mxk[i] = max(mxk[i], __shfl_sync(grp, mx_self[i], src));
-                }
-            }
-        }
-        if (node >= 0 && lane == leader) {
-            atomicMax(b.r2 + node, __float_as_uint(acc_r2));  // non-negative floats
-            for (int i = 0; i < 6; i++) atomicAdd(b.q + 6 * (int64_t)node + i, acc_q[i]);
+        } else {  // several nodes: segmented over the warp's runs
+            const WarpRuns r = warp_runs(node);
+            v[0] = run_scan(v[0], r, FMaxOp());
+            for (int i = 1; i < 7; i++) v[i] = run_scan(v[i], r, AddOp());
             for (int i = 0; i < 3; i++) {
-                atomicMin(b.box + 6 * (int64_t)node + i, mn[i]);
-                atomicMax(b.box + 6 * (int64_t)node + 3 + i, mxk[i]);
+                bx[i] = run_scan(bx[i], r, MinOp());
+                bx[3 + i] = run_scan(bx[3 + i], r, MaxOp());
+            }
+            if (r.tail && node >= 0) {
+                atomicMax(b.r2 + node, __float_as_uint(v[0]));  // non-negative floats
+                for (int i = 0; i < 6; i++) atomicAdd(b.q + 6 * (int64_t)node + i, v[1 + i]);
+                for (int i = 0; i < 3; i++) {
+                    atomicMin(b.box + 6 * (int64_t)node + i, bx[i]);
+                    atomicMax(b.box + 6 * (int64_t)node + 3 + i, bx[3 + i]);
+                }
             }
         }
-        // octant counts: lanes sharing (node, key)
-        const unsigned g2 = __match_any_sync(0xffffffffu, node * 8 + key);
-        if (node >= 0 && lane == __ffs(g2) - 1) atomicAdd(b.oct + 8 * (int64_t)node + key, __popc(g2));
+        if (block_uniform) {  // then over the block: one atomic per value
+            if (lane == 0) {
+                for (int i = 0; i < 7; i++) s_f[i][warp] = v[i];
+                for (int i = 0; i < 6; i++) s_k[i][warp] = bx[i];
+            }
+            const unsigned g2 = __match_any_sync(0xffffffffu, key);
+            if (lane == __ffs(g2) - 1) atomicAdd(s_oct + key, __popc(g2));
+            __syncthreads();
+            if (threadIdx.x < 7) {
+                const int i = threadIdx.x;
+                float a = s_f[i][0];
+                for (int w2 = 1; w2 < kWarps; w2++) a = i == 0 ? fmaxf(a, s_f[i][w2]) : a + s_f[i][w2];
+                if (i == 0) atomicMax(b.r2 + s_node, __float_as_uint(a));
+                else atomicAdd(b.q + 6 * (int64_t)s_node + (i - 1), a);
+            } else if (threadIdx.x < 13) {
+                const int i = threadIdx.x - 7;
+                unsigned a = s_k[i][0];
+                for (int w2 = 1; w2 < kWarps; w2++) a = i < 3 ? min(a, s_k[i][w2]) : max(a, s_k[i][w2]);
+                if (i < 3) atomicMin(b.box + 6 * (int64_t)s_node + i, a);
+                else atomicMax(b.box + 6 * (int64_t)s_node + i, a);
+            } else if (threadIdx.x >= 32 && threadIdx.x < 40) {
+                const int c = threadIdx.x - 32;
+                if (s_oct[c]) atomicAdd(b.oct + 8 * (int64_t)s_node + c, s_oct[c]);
+                s_oct[c] = 0;
+            }
+        } else {
+            if (warp_uniform && node >= 0 && lane == 0) {
+                atomicMax(b.r2 + node, __float_as_uint(v[0]));
+                for (int i = 0; i < 6; i++) atomicAdd(b.q + 6 * (int64_t)node + i, v[1 + i]);
+                for (int i = 0; i < 3; i++) {
+                    atomicMin(b.box + 6 * (int64_t)node + i, bx[i]);
+                    atomicMax(b.box + 6 * (int64_t)node + 3 + i, bx[3 + i]);
+                }
+            }
+            // octant counts: lanes sharing (node, key)
+            const unsigned g2 = __match_any_sync(0xffffffffu, node * 8 + key);
+            if (node >= 0 && lane == __ffs(g2) - 1) atomicAdd(b.oct + 8 * (int64_t)node + key, __popc(g2));
+        }
+        __syncthreads();  // s_node, s_f, s_k and s_oct are reused by the next iteration
     }
 }
 

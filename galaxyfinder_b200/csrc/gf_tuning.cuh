@@ -43,6 +43,9 @@
 #ifndef GF_BH_ACC      // Barnes-Hut sums: 0 = FP32 with Kahan compensation, 1 = FP64
 #define GF_BH_ACC 0
 #endif
+#ifndef GF_KNNB_WIN    // float-key kNN: nodes staged per warp in shared memory (0, 8, 16 or 32)
+#define GF_KNNB_WIN 32
+#endif
 #ifndef GF_KNNB_DYN    // float-key kNN: 1 = warps take buckets from a work counter, 0 = grid-stride
 #define GF_KNNB_DYN 0
 #endif
@@ -76,6 +79,7 @@ static_assert(GF_KNNB_SEEDS >= 32 && GF_KNNB_SEEDS % 2 == 0, "GF_KNNB_SEEDS");
 static_assert(GF_BH_BLOCK % 32 == 0 && GF_BH_BLOCK <= 1024, "GF_BH_BLOCK");
 static_assert(GF_BH_DYN == 0 || GF_BH_DYN == 1, "GF_BH_DYN");
 static_assert(GF_KNNB_DYN == 0 || GF_KNNB_DYN == 1, "GF_KNNB_DYN");
+static_assert(GF_KNNB_WIN == 0 || GF_KNNB_WIN == 8 || GF_KNNB_WIN == 16 || GF_KNNB_WIN == 32, "GF_KNNB_WIN");
 static_assert(GF_BH_ACC == 0 || GF_BH_ACC == 1, "GF_BH_ACC");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");
 static_assert(GF_FFT_PENCILS_64 >= 32 && GF_FFT_PENCILS_64 <= 128 &&

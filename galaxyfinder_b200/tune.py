@@ -12,10 +12,11 @@ the GPU and the workload), which build.py turns into -D flags.
 
   group   parameters                                   phase
   knn     GF_KNN_ALGO x GF_KNNB_BLOCK (x GF_KNNB_ARITY), then GF_KNNB_SEEDS,
-          GF_KNNB_LANECERT and GF_KNNB_QUEUE for the
+          GF_KNNB_LANECERT, GF_KNNB_DYN, GF_KNNB_WIN x GF_KNNB_MINB
+          (node window against resident blocks) and GF_KNNB_QUEUE for the
           float-key kernel; for the warp-per-query
           kernel GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
-  bh      GF_BH_BLOCK, then the register cap           potential
+  bh      GF_BH_DYN, GF_BH_ACC, GF_BH_BLOCK, then the register cap   potential
   fft     GF_FFT_PENCILS                               smooth
   tsc     GF_TSC_TILE (0: direct global atomics)       tsc
   tree    GF_TREE_BLOCK                                tree
@@ -40,7 +41,7 @@ from . import build as B
 TUNE_DIR = B.PKG / "_tune"
 DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0, "GF_KNNB_LANECERT": 0,
             "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
-            "GF_BH_BLOCK": 128, "GF_BH_DYN": 0, "GF_BH_ACC": 0, "GF_KNNB_DYN": 0,
+            "GF_BH_BLOCK": 128, "GF_BH_DYN": 0, "GF_BH_ACC": 0, "GF_KNNB_DYN": 0, "GF_KNNB_WIN": 32, "GF_KNNB_MINB": 1,
             "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TSC_TILE": 0, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
 
@@ -59,6 +60,8 @@ def stages(group: str):
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_SEEDS": n} for n in (32, 48, 64, 80, 96)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_LANECERT": c} for c in (0, 1)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_DYN": d} for d in (0, 1)],
+                lambda base: [] if base["GF_KNN_ALGO"] != 2 else
+                [{"GF_KNNB_WIN": w, "GF_KNNB_MINB": mb} for w, mb in ((32, 1), (8, 6), (0, 6), (0, 1))],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_QUEUE": q} for q in (0, 2, 4, 8)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else
@@ -84,7 +87,11 @@ GROUPS = {"knn": ("gf_knn.cu", "knn"), "bh": ("gf_potent.cu", "potential"),
 
 
 def variant_name(params: dict) -> str:
-    return "_".join(f"{k[3:].lower()}{v}" for k, v in sorted(params.items()))
+    name = "_".join(f"{k[3:].lower()}{v}" for k, v in sorted(params.items()))
+    if len(name) > 160:  # a directory name: keep it short, and unique by digest
+        import hashlib
+        name = "v" + hashlib.sha1(name.encode()).hexdigest()[:16]
+    return name
 
 
 def build_variant(src_name: str, params: dict) -> Path:
