@@ -331,7 +331,8 @@ int gf_tuning_value(const char *name, int64_t *value) {
                   {"GF_FFT_PENCILS", GF_FFT_PENCILS}, {"GF_TREE_BLOCK", GF_TREE_BLOCK},
                   {"GF_KNNB_QUEUE", GF_KNNB_QUEUE},   {"GF_KNNB_LANECERT", GF_KNNB_LANECERT},
                   {"GF_BH_DYN", GF_BH_DYN},           {"GF_KNNB_DYN", GF_KNNB_DYN},
-                  {"GF_BH_ACC", GF_BH_ACC},
+                  {"GF_BH_ACC", GF_BH_ACC},           {"GF_KNNB_WIN", GF_KNNB_WIN},
+                  {"GF_KNNB_MINB", GF_KNNB_MINB},
                   {"GF_FFT_PENCILS_64", GF_FFT_PENCILS_64},
                   {"GF_FFT_PENCILS_128", GF_FFT_PENCILS_128}, {"GF_TSC_TILE", GF_TSC_TILE}};
     if (!name || !value) return GF_EINVAL;

@@ -18,8 +18,14 @@ def _valid(p):
     assert p["GF_FFT_PENCILS_64"] in (32, 64, 128) and p["GF_FFT_PENCILS_128"] in (32, 64)
     assert 128 <= p["GF_TREE_BLOCK"] <= 1024
     assert p["GF_TSC_TILE"] == 0 or 1024 <= p["GF_TSC_TILE"] <= 12288
-    for b, m in ((p["GF_KNN_BLOCK"], p["GF_KNN_MINB"]), (p["GF_BH_BLOCK"], p["GF_BH_MINB"])):
+    assert p["GF_KNNB_WIN"] in (0, 8, 16, 32)
+    for b, m in ((p["GF_KNN_BLOCK"], p["GF_KNN_MINB"]), (p["GF_BH_BLOCK"], p["GF_BH_MINB"]),
+                 (p["GF_KNNB_BLOCK"], p["GF_KNNB_MINB"])):
         assert m >= 1 and b * m <= 2048  # resident threads per SM
+    # the float-key kernel's shared memory per warp: heaps, node window, tile
+    warp_bytes = 32 * 32 * 8 + p["GF_KNNB_WIN"] * 48 + 32 * 16 + 32 * 4 + 32 * p["GF_KNNB_QUEUE"] * 8
+    if p["GF_KNN_ALGO"] == 2:
+        assert p["GF_KNNB_MINB"] * (p["GF_KNNB_BLOCK"] // 32 * warp_bytes + 1024) <= 228 * 1024
 
 
 def test_search_space_is_valid():
@@ -37,8 +43,9 @@ def test_search_space_is_valid():
         assert len(T.stages("knn")[1](base)) == (5 if algo == 2 else 0)  # seed windows
         assert len(T.stages("knn")[2](base)) == (2 if algo == 2 else 0)  # lane or warp certification
         assert len(T.stages("knn")[3](base)) == (2 if algo == 2 else 0)  # work counter or grid-stride
-        assert len(T.stages("knn")[4](base)) == (4 if algo == 2 else 0)  # survivor queues
-        assert len(T.stages("knn")[5](base)) == (3 if algo == 0 else 0)
+        assert len(T.stages("knn")[4](base)) == (4 if algo == 2 else 0)  # node window x resident blocks
+        assert len(T.stages("knn")[5](base)) == (4 if algo == 2 else 0)  # survivor queues
+        assert len(T.stages("knn")[6](base)) == (3 if algo == 0 else 0)
 
 
 def test_tuned_params_become_flags(tmp_path, monkeypatch):
@@ -56,7 +63,8 @@ def test_library_reports_its_launch_parameters():
     with; build.py compiles with tuned.json's values."""
     from galaxyfinder_b200 import _lib
     params = B.tuned_params()
-    for name in ("GF_KNN_ALGO", "GF_KNNB_BLOCK", "GF_KNNB_SEEDS", "GF_BH_BLOCK", "GF_FFT_PENCILS"):
+    for name in ("GF_KNN_ALGO", "GF_KNNB_BLOCK", "GF_KNNB_SEEDS", "GF_BH_BLOCK", "GF_FFT_PENCILS", "GF_KNNB_WIN",
+                 "GF_KNNB_MINB", "GF_BH_DYN", "GF_KNNB_DYN"):
         assert _lib.tuning_value(name) == params.get(name, T.DEFAULTS[name]), name
     import pytest
     with pytest.raises(_lib.GFError):
