@@ -42,13 +42,15 @@ UNIT = "particles/s"
 K_NEIGH = 32
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per particle of
-# each phase's dominant kernel, from one ncu capture of the 256-halo catalogue
-# (201,933 particles); the traffic scales with the particles processed.
-TRAFFIC_PER_PARTICLE = {"knn": (9.436672e6 + 1.536e3) / 201933}
+# each phase's dominant kernel, from one ncu capture of the 1024-halo
+# catalogue (1,281,067 particles); the traffic scales with the particles
+# processed.
+TRAFFIC_PER_PARTICLE = {"knn": (60.081152e6 + 115.645e6) / 1281067}
 # What bounds the kNN kernel instead of HBM, from the same capture: the tree
-# walk is latency- and issue-bound (its HBM traffic is a few bytes per query).
-KNN_LIMITER = ("latency/issue: 58.8% of issue slots active, 24.9% of warp slots occupied (shared-memory "
-               "heaps limit residency to 20 warps/SM), dominant stall 'wait'; DRAM 0.12% of peak")
+# walk is latency- and issue-bound (its HBM traffic is the neighbour lists).
+KNN_LIMITER = ("latency/issue: 68.7% of issue slots active, 36.0% of warp slots occupied (6 blocks of 4 "
+               "warps per SM: 79 registers and 35.3 KB of heaps per block), dominant stall 'wait'; "
+               "DRAM 0.64% of peak")
 
 
 def parse():
@@ -860,7 +862,7 @@ def main():
         roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"],
                     "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                     "traffic": None if traffic is None else traffic * n,
-                    "traffic_note": "bytes per launch, ncu capture of the 256-halo catalogue scaled by particles",
+                    "traffic_note": "bytes per launch, ncu capture of the 1024-halo catalogue scaled by particles",
                     "algorithmic_bytes": alg[dom], "peak_source": pk["source"]}
         if dom == "knn":
             roofline["limiter"] = KNN_LIMITER
@@ -897,7 +899,7 @@ def main():
     line = dict(base)
     line.update({
         "value": head["value"], "ms_per_step": head["ms_per_step"],
-        "config": dict(workload_config(args, hb, world, int(cells)), graph=use_graph),
+        "config": workload_config(args, hb, world, int(cells)),  # the same object as the reference arm's
         "pipeline": (f"{nchunks} halo chunks on their own streams and host threads"
                      + (", each replaying its stage captured as one CUDA graph" if use_graph else "")),
         "tree_nodes": int(st["nnode"]),

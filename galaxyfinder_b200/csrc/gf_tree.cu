@@ -412,12 +412,17 @@ __global__ void split_nodes(int L, int32_t ncap, int last, Build b) {
     }
 }
 
+// Moves the active particles into [loose | child 0 | child 1 | ...] order.
+// A particle that stays loose here has its final tree-order slot: it is
+// written once into the final arrays (fpos, fperm) and never copied again;
+// its slot, like every earlier-settled one, carries node -1 into the next
+// level.
 __global__ void scatter_particles(int64_t n, const float4 *__restrict__ pos_in,
                                   const int32_t *__restrict__ perm_in,
                                   const int32_t *__restrict__ pnode_in,
                                   const uint8_t *__restrict__ pkey, float4 *__restrict__ pos_out,
                                   int32_t *__restrict__ perm_out, int32_t *__restrict__ pnode_out,
-                                  Build b) {
+                                  float4 *__restrict__ fpos, int32_t *__restrict__ fperm, Build b) {
     const int lane = threadIdx.x & 31;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p - lane < n;
          p += (int64_t)gridDim.x * blockDim.x) {
@@ -425,9 +430,7 @@ __global__ void scatter_particles(int64_t n, const float4 *__restrict__ pos_in,
         const int key = node >= 0 ? pkey[p] : 0;
         const unsigned g = __match_any_sync(0xffffffffu, node * 8 + key);
         if (p >= n) continue;
-        if (node < 0) {  // settled earlier: stays in place
-            pos_out[p] = pos_in[p];
-            perm_out[p] = perm_in[p];
+        if (node < 0) {  // settled at an earlier level: already in the final arrays
             pnode_out[p] = -1;
             continue;
         }
@@ -436,9 +439,15 @@ __global__ void scatter_particles(int64_t n, const float4 *__restrict__ pos_in,
         if (lane == leader) base = atomicAdd(b.cur + 8 * (int64_t)node + key, __popc(g));
         base = __shfl_sync(g, base, leader);
         const int dest = base + __popc(g & ((1u << lane) - 1));
-        pos_out[dest] = pos_in[p];
-        perm_out[dest] = perm_in[p];
-        pnode_out[dest] = b.ochild[8 * (int64_t)node + key];
+        const int child = b.ochild[8 * (int64_t)node + key];
+        if (child >= 0) {
+            pos_out[dest] = pos_in[p];
+            perm_out[dest] = perm_in[p];
+        } else {
+            fpos[dest] = pos_in[p];
+            fperm[dest] = perm_in[p];
+        }
+        pnode_out[dest] = child;
     }
 }
 
@@ -582,13 +591,15 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
     for (int attempt = 0; attempt < (fixed ? 1 : 4); attempt++, ncap *= 2) {
         // ---- particle buffers: pos x2, perm x2, pnode x2, key
         auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
-        const size_t pbytes = 2 * al(n * sizeof(float4)) + 4 * al(n * sizeof(int32_t)) + al(n);
+        const size_t pbytes = 3 * al(n * sizeof(float4)) + 5 * al(n * sizeof(int32_t)) + al(n);
         GF_TRY(ctx->tree[0].reserve(pbytes + 256));
         char *pp = ctx->tree[0].as<char>();
         float4 *pos[2] = {carve<float4>(pp, n), carve<float4>(pp, n)};
         int32_t *perm[2] = {carve<int32_t>(pp, n), carve<int32_t>(pp, n)};
         int32_t *pnode[2] = {carve<int32_t>(pp, n), carve<int32_t>(pp, n)};
         uint8_t *pkey = carve<uint8_t>(pp, n);
+        float4 *fpos = carve<float4>(pp, n);    // final tree order, written as particles settle
+        int32_t *fperm = carve<int32_t>(pp, n);
         // ---- node buffers (BFS numbering): exactly the carves below
         const size_t nc = (size_t)ncap;
         const size_t nbytes = 3 * al(nc * 4) + 4 * al(nc * 8) + al(nc * 4) + al(nc * 24) +
@@ -663,7 +674,7 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
             GF_LAUNCH_CHECK();
             scatter_particles<<<grid_n(n), kBlock, 0, s>>>(n, pos[cur], perm[cur], pnode[cur], pkey,
                                                            pos[cur ^ 1], perm[cur ^ 1],
-                                                           pnode[cur ^ 1], b);
+                                                           pnode[cur ^ 1], fpos, fperm, b);
             GF_LAUNCH_CHECK();
             cur ^= 1;
             nlev = L + 1;
@@ -725,8 +736,8 @@ int build_tree(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t *pstart_dev,
         out->nhalo = nhalo;
         out->nnode = nnode;
         out->n = n;
-        out->pos = pos[cur];
-        out->perm = perm[cur];
+        out->pos = fpos;
+        out->perm = fperm;
         out->root = root;
         out->rend = rend;
         out->knn = knn;
