@@ -289,7 +289,9 @@ int gf_plan_meshes(int32_t nhalo, const double *extent, const gf_mesh_rule *rule
  * 1024 cells (GF_EINVAL otherwise).  The first call on a device looks up the
  * array's device address with that device current, so make it before any
  * stream capture.  All calls share the array: calls that may overlap on the
- * GPU (different streams without ordering) race and must be serialised. */
+ * GPU (different streams without ordering) race and must be serialised.
+ * Every call plans on the host; an axis whose length is not a power of two
+ * takes its exact n-tap filter from an O(n^2) FP64 sum there. */
 int gf_gaussian_smooth_noalloc(float *den, int nx, int ny, int nz, double cellsize, float RG,
                                void *stream);
 
