@@ -162,6 +162,10 @@ int check_device_errors(gf_ctx *ctx) {
             set_status(GF_EINVAL, "a kNN query found fewer neighbours than requested");
             return GF_EINVAL;
         }
+        if (h & GF_ERRBIT_WAIT) {
+            set_status(GF_ETIMEOUT, "an asynchronous copy did not complete within its wait bound");
+            return GF_ETIMEOUT;
+        }
         if (h & GF_ERRBIT_WALK) {
             set_status(GF_ETIMEOUT, "a tree walk exceeded its step bound");
             return GF_ETIMEOUT;
@@ -332,7 +336,7 @@ int gf_tuning_value(const char *name, int64_t *value) {
                   {"GF_KNNB_QUEUE", GF_KNNB_QUEUE},   {"GF_KNNB_LANECERT", GF_KNNB_LANECERT},
                   {"GF_BH_DYN", GF_BH_DYN},           {"GF_KNNB_DYN", GF_KNNB_DYN},
                   {"GF_BH_ACC", GF_BH_ACC},           {"GF_KNNB_WIN", GF_KNNB_WIN},
-                  {"GF_KNNB_MINB", GF_KNNB_MINB},
+                  {"GF_KNNB_MINB", GF_KNNB_MINB},     {"GF_BH_TMA", GF_BH_TMA},
                   {"GF_FFT_PENCILS_64", GF_FFT_PENCILS_64},
                   {"GF_FFT_PENCILS_128", GF_FFT_PENCILS_128}, {"GF_TSC_TILE", GF_TSC_TILE}};
     if (!name || !value) return GF_EINVAL;

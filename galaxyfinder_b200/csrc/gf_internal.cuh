@@ -63,6 +63,7 @@ enum : int {
     GF_ERRBIT_WALK = 8,       // a tree walk exceeded its step bound
     GF_ERRBIT_INDEX = 16,     // an index argument (query, neighbour) is out of range
     GF_ERRBIT_PLAN = 32,      // the batch no longer fits a captured stage plan
+    GF_ERRBIT_WAIT = 64,      // a bounded wait for an asynchronous copy ran out
 };
 
 // ---------------------------------------------------------------- workspace

@@ -68,6 +68,55 @@ __device__ double bg_potent_dev(double mvir, const PotentialParams &pp) {
     return vc2 * (1 - gc * log(1 + c));
 }
 
+// ---- leaf tiles staged by the bulk-copy (TMA) engine, GF_BH_TMA=1
+// When lanes open a node whose loose particles fit a slot (at most
+// kLeafSlotP float4), one lane has the tensor-memory-access unit copy them
+// (cp.async.bulk, global -> this CTA's shared memory, completion counted on
+// an mbarrier; no multicast) into the next slot of a per-warp ring, and the
+// warp walks on; the opened leaf is summed from shared memory later, when the
+// ring is full or the walk ends.  Every wait is bounded: a copy that does not
+// complete in time sets GF_ERRBIT_WAIT and the warp falls back to global
+// loads for the rest of the launch.
+constexpr int kLeafSlots = 4;   // ring slots per warp
+constexpr int kLeafSlotP = 32;  // float4 (particles) per slot
+constexpr int kWaitTries = 1 << 20;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// bytes: a multiple of 16; src and dst 16-byte aligned
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    uint64_t g;
+    asm("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(src));
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(g), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// the generic-proxy reads of a slot precede the async-proxy write that reuses it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // COUNT: interaction counters (bench and tests); off in the stage's walk.
 template <bool COUNT>
 __global__ void __launch_bounds__(GF_BH_BLOCK, GF_BH_MINB)
@@ -77,8 +126,24 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
           const BhNode *__restrict__ nodes, const int32_t *__restrict__ direct,
           const double *__restrict__ bg, PotentialParams pp, float *__restrict__ out,
           float *__restrict__ raw, unsigned long long *__restrict__ counters,
-          unsigned long long *__restrict__ work) {
+          unsigned long long *__restrict__ work, int *__restrict__ err) {
     const int lane = threadIdx.x & 31;
+#if GF_BH_TMA
+    __shared__ __align__(16) float4 leaf_ring[GF_BH_BLOCK / 32][kLeafSlots][kLeafSlotP];
+    __shared__ __align__(8) uint64_t leaf_bar[GF_BH_BLOCK / 32][kLeafSlots];
+    float4(*ring)[kLeafSlotP] = leaf_ring[threadIdx.x >> 5];
+    uint64_t *bars = leaf_bar[threadIdx.x >> 5];
+    if (lane < kLeafSlots) mbar_init(bars + lane);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncwarp();
+    uint32_t phases = 0;        // parity each slot's barrier completes next (warp-uniform)
+    int head = 0, pending = 0;  // oldest staged slot, staged slots (warp-uniform)
+    unsigned qmask = 0;         // in lane s < kLeafSlots: the lanes that opened slot s's leaf
+    int qcnt = 0;               // in lane s: the particles in slot s
+    bool tma_ok = true;         // cleared by a wait that ran out
+#else
+    (void)err;
+#endif
     const int64_t warp0 = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32;
     const int64_t wstride = (int64_t)gridDim.x * blockDim.x;
     unsigned long long npp = 0, npc = 0;
@@ -104,9 +169,46 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
         }
         const double px = P.x, py = P.y, pz = P.z;
         BhAcc acc;
+        // ost.c:186-191: float offsets of the two positions.  For float
+        // inputs the FP32 difference is the correctly rounded exact
+        // difference, i.e. the same bits as rounding the FP64 difference.
+        auto particle_term = [&](const float4 &S) {
+            const float fx = P.x - S.x;
+            const float fy = P.y - S.y;
+            const float fz = P.z - S.z;
+            const float r2 = fx * fx + fy * fy + fz * fz;
+            if (r2 > 0.f) acc.add(-S.w * rsqrtf(r2));
+        };
+#if GF_BH_TMA
+        // sums the oldest staged leaf once its copy has landed
+        auto consume = [&]() {
+            const int slot = head;
+            const uint32_t par = (phases >> slot) & 1u;
+            bool ok = false;
+            for (int it = 0; it < kWaitTries && !ok; it++) ok = mbar_try_wait(bars + slot, par);
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) atomicOr(err, GF_ERRBIT_WAIT);
+                // the copy may still land in this slot: wait for it once
+                // more, then stage no further leaves in this launch
+                ok = false;
+                for (int it = 0; it < kWaitTries && !ok; it++) ok = mbar_try_wait(bars + slot, par);
+                tma_ok = false;
+            }
+            phases ^= 1u << slot;
+            const unsigned m = __shfl_sync(0xffffffffu, qmask, slot);
+            const int c = __shfl_sync(0xffffffffu, qcnt, slot);
+            if ((m >> lane) & 1u)
+                for (int j = 0; j < c; j++) particle_term(ring[slot][j]);
+            __syncwarp();  // every lane's reads of the slot precede its next copy
+            head = (head + 1) % kLeafSlots;
+            pending--;
+        };
+#endif
         while (true) {
             const int i = (int)__reduce_min_sync(0xffffffffu, (unsigned)my);
             if (i == INT_MAX) break;
+            bool stage = false;  // this lane opened a leaf that is staged
+            int stage_l0 = 0, stage_n = 0;
             if (my == i) {
                 // the node in 16-byte words: (com x, com y), (com z, open_r2),
                 // (mass, trq, qxx, qyy), (qzz, qxy, qxz, qyz), (skip, lstart, lcount, count)
@@ -125,18 +227,16 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
                 const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
                                             __dmul_rn(dz, dz));
                 if (always_open || d2 < c2r.y) {
-                    const int l1 = links.y + links.z;
-                    for (int j = links.y; j < l1; j++) {
-                        const float4 S = spos[j];
-                        // ost.c:186-191: float offsets of the two positions.  For
-                        // float inputs the FP32 difference is the correctly
-                        // rounded exact difference, i.e. the same bits as
-                        // rounding the FP64 difference.
-                        const float fx = P.x - S.x;
-                        const float fy = P.y - S.y;
-                        const float fz = P.z - S.z;
-                        const float r2 = fx * fx + fy * fy + fz * fz;
-                        if (r2 > 0.f) acc.add(-S.w * rsqrtf(r2));
+#if GF_BH_TMA
+                    if (tma_ok && links.z > 0 && links.z <= kLeafSlotP) {
+                        stage = true;
+                        stage_l0 = links.y;
+                        stage_n = links.z;
+                    } else
+#endif
+                    {
+                        const int l1 = links.y + links.z;
+                        for (int j = links.y; j < l1; j++) particle_term(spos[j]);
                     }
                     if (COUNT) npp += links.z;
                     my = i + 1;
@@ -154,7 +254,30 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
                 }
                 if (my >= my_end) my = INT_MAX;
             }
+#if GF_BH_TMA
+            const unsigned om = __ballot_sync(0xffffffffu, stage);
+            if (om) {  // the lanes at node i that opened it share its loose particles
+                const int src = __ffs(om) - 1;
+                const int l0 = __shfl_sync(0xffffffffu, stage_l0, src);
+                const int nl = __shfl_sync(0xffffffffu, stage_n, src);
+                if (pending == kLeafSlots) consume();
+                const int slot = (head + pending) % kLeafSlots;
+                if (lane == 0) {
+                    fence_proxy_async_smem();
+                    mbar_expect_tx(bars + slot, (uint32_t)nl * 16u);
+                    bulk_copy_g2s(ring[slot], spos + l0, (uint32_t)nl * 16u, bars + slot);
+                }
+                if (lane == slot) {
+                    qmask = om;
+                    qcnt = nl;
+                }
+                pending++;
+            }
+#endif
         }
+#if GF_BH_TMA
+        while (pending) consume();  // the walk's staged leaves, before the outputs
+#endif
         if (valid) {
             const int64_t o = tout ? tout[t] : t;
             const float phi = acc.value();
@@ -201,7 +324,7 @@ int launch_bh(gf_ctx *ctx, int64_t grid, int64_t ntarget, const float4 *tpos, co
         GF_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(unsigned long long), ctx->stream));
     }
     kern<<<(int)grid, block, 0, ctx->stream>>>(ntarget, tpos, thalo, tout, spos, root, rend, nodes, direct, bg, pp,
-                                               out, raw, counters, work);
+                                               out, raw, counters, work, ctx->d_err);
     GF_LAUNCH_CHECK();
     return GF_OK;
 }

@@ -40,6 +40,9 @@
 #ifndef GF_BH_DYN      // Barnes-Hut walk: 1 = warps take targets from a work counter, 0 = grid-stride
 #define GF_BH_DYN 0
 #endif
+#ifndef GF_BH_TMA      // Barnes-Hut walk: 1 = opened leaves staged in shared memory by bulk copies
+#define GF_BH_TMA 0
+#endif
 #ifndef GF_BH_ACC      // Barnes-Hut sums: 0 = FP32 with Kahan compensation, 1 = FP64
 #define GF_BH_ACC 0
 #endif
@@ -81,6 +84,7 @@ static_assert(GF_BH_DYN == 0 || GF_BH_DYN == 1, "GF_BH_DYN");
 static_assert(GF_KNNB_DYN == 0 || GF_KNNB_DYN == 1, "GF_KNNB_DYN");
 static_assert(GF_KNNB_WIN == 0 || GF_KNNB_WIN == 8 || GF_KNNB_WIN == 16 || GF_KNNB_WIN == 32, "GF_KNNB_WIN");
 static_assert(GF_BH_ACC == 0 || GF_BH_ACC == 1, "GF_BH_ACC");
+static_assert(GF_BH_TMA == 0 || GF_BH_TMA == 1, "GF_BH_TMA");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");
 static_assert(GF_FFT_PENCILS_64 >= 32 && GF_FFT_PENCILS_64 <= 128 &&
                   (GF_FFT_PENCILS_64 & (GF_FFT_PENCILS_64 - 1)) == 0, "GF_FFT_PENCILS_64");

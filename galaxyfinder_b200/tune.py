@@ -16,7 +16,8 @@ the GPU and the workload), which build.py turns into -D flags.
           (node window against resident blocks) and GF_KNNB_QUEUE for the
           float-key kernel; for the warp-per-query
           kernel GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
-  bh      GF_BH_DYN, GF_BH_ACC, GF_BH_BLOCK, then the register cap   potential
+  bh      GF_BH_DYN, GF_BH_ACC, GF_BH_TMA (leaf staging), GF_BH_BLOCK,
+          then the register cap                        potential
   fft     GF_FFT_PENCILS                               smooth
   tsc     GF_TSC_TILE (0: direct global atomics)       tsc
   tree    GF_TREE_BLOCK                                tree
@@ -41,7 +42,7 @@ from . import build as B
 TUNE_DIR = B.PKG / "_tune"
 DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0, "GF_KNNB_LANECERT": 0,
             "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
-            "GF_BH_BLOCK": 128, "GF_BH_DYN": 0, "GF_BH_ACC": 0, "GF_KNNB_DYN": 0, "GF_KNNB_WIN": 32, "GF_KNNB_MINB": 1,
+            "GF_BH_BLOCK": 128, "GF_BH_DYN": 0, "GF_BH_ACC": 0, "GF_BH_TMA": 0, "GF_KNNB_DYN": 0, "GF_KNNB_WIN": 32, "GF_KNNB_MINB": 1,
             "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TSC_TILE": 0, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
 
@@ -69,6 +70,7 @@ def stages(group: str):
     if group == "bh":
         return [lambda base: [{"GF_BH_DYN": d} for d in (0, 1)],
                 lambda base: [{"GF_BH_ACC": a} for a in (0, 1)],
+                lambda base: [{"GF_BH_TMA": t} for t in (0, 1)],
                 lambda base: [{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],
                 lambda base: [{"GF_BH_MINB": minb(base["GF_BH_BLOCK"], r)} for r in REGCAPS]]
     if group == "fft":

@@ -19,6 +19,7 @@ def _valid(p):
     assert 128 <= p["GF_TREE_BLOCK"] <= 1024
     assert p["GF_TSC_TILE"] == 0 or 1024 <= p["GF_TSC_TILE"] <= 12288
     assert p["GF_KNNB_WIN"] in (0, 8, 16, 32)
+    assert p["GF_BH_TMA"] in (0, 1)
     for b, m in ((p["GF_KNN_BLOCK"], p["GF_KNN_MINB"]), (p["GF_BH_BLOCK"], p["GF_BH_MINB"]),
                  (p["GF_KNNB_BLOCK"], p["GF_KNNB_MINB"])):
         assert m >= 1 and b * m <= 2048  # resident threads per SM
