@@ -222,6 +222,11 @@ SIGNATURES = {
                              ctypes.POINTER(_I64)]),
     "gf_self_potential": (_INT, [_VP, _I32, _I64, _VP, _VP, _F, _I32, _D, _INT, _VP, _VP]),
     "gf_bg_potent_device": (_INT, [_VP, _I32, _VP, _VP]),
+    "mkRtidal": (None, []),
+    "nfw_rtidal": (_F, [_F, _F, _F]),
+    "gf_nfw_rtidal_cells": (_INT, []),
+    "gf_nfw_rtidal_table": (_INT, [_VP, _VP]),
+    "gf_nfw_rtidal_lookup": (_INT, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
     "gf_stage_run": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),
                             ctypes.POINTER(StageOut), ctypes.POINTER(StageStats)]),
     "gf_stage_graph_create": (_INT, [_VP, ctypes.POINTER(Batch), ctypes.POINTER(StageConfig),

@@ -168,6 +168,14 @@ int CheckExternalTE(Kptype *tkp, int tnp, unsigned char *bndflag, Kptype *skp, i
  * kernel -1/r and its quadrupole terms exactly, so no table is built; the
  * call only initialises the device. */
 void i_potent_spline(void);
+/* NewGalFinder/mkRtidal.c:80.  Builds the NFW tidal-radius table of the
+ * OLD_TIDAL build (32 concentrations x 128 distances x 128 mass ratios) on
+ * the GPU into the library's copy that nfw_rtidal reads. */
+void mkRtidal(void);
+/* NewGalFinder/mkRtidal.c:60.  The table entry of (satellite / host mass
+ * ratio, distance in host virial radii, host concentration): the tidal radius
+ * in units of the distance; 0 before mkRtidal has run. */
+float nfw_rtidal(float mM, float dRv, float c);
 
 /* Tidal radius of every core: AdGetTidalRCenterCore (subhaloden.mod6.c:1910-2035)
  * with get_tidal_ellipse (:1102-1165).  The reference reads each particle's
@@ -423,6 +431,15 @@ int gf_knn_density_adjoint(gf_ctx *ctx, int32_t nhalo, int64_t n, const int64_t 
  * x87 long double, so its intermediates are double where the reference's
  * (and gf_bg_potent's) are long double. */
 int gf_bg_potent_device(gf_ctx *ctx, int32_t n, const double *mvir_dev, double *bg_dev);
+/* The NFW tidal-radius table of mkRtidal (mkRtidal.c:80-128) into a device
+ * buffer of gf_nfw_rtidal_cells() floats, laid out as the reference's
+ * tidal_den (mass ratio fastest, then distance, then concentration); and
+ * nfw_rtidal (mkRtidal.c:60-78) for n (mass ratio, distance / Rvir, c)
+ * triples of device arrays on such a table.  Stream ordered on ctx. */
+int gf_nfw_rtidal_cells(void);
+int gf_nfw_rtidal_table(gf_ctx *ctx, float *table_dev);
+int gf_nfw_rtidal_lookup(gf_ctx *ctx, int64_t n, const float *mM_dev, const float *dRv_dev,
+                         const float *c_dev, const float *table_dev, float *out_dev);
 /* Self potential of every halo: penergy = phi * potentfact + bg(halo mass)
  * (bg only if add_bg); halos with fewer than ndirect particles are summed
  * directly.  raw (optional) receives phi itself. */
