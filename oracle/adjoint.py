@@ -1,5 +1,5 @@
 """FP64 restatement of the differentiable density stage and of its gradient
-(test infrastructure only; used by tests/ as the checker).
+(test infrastructure only; tests/ check results against it).
 
 Everything here is plain FP64 numpy, with no float rounding anywhere, so
 that central finite differences with h = 1e-6 are meaningful:

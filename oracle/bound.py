@@ -1,5 +1,5 @@
 """CPU restatement of NewGalFinder's boundedness test, tidal radius and tidal
-cut (test infrastructure only; used by tests/ as the checker).
+cut (test infrastructure only; tests/ check results against it).
 
 The reference mixes float, double and long double in these routines; the
 restatement keeps each operand type:

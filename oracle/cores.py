@@ -1,5 +1,5 @@
 """CPU restatement of the reference's core finding on the kNN graph (test
-infrastructure only: the checker of libgf's gf_density_peaks / gf_core_density
+infrastructure only: the reference results for libgf's gf_density_peaks / gf_core_density
 and of the finddenpeak / FindCoreDensity drop-ins).
 
 * density_peaks follows NewGalFinder/subhaloden.mod6.c:416-494 (finddenpeak):

@@ -1,7 +1,7 @@
 /* CPU restatement of the reference's density-and-potential stage — the oracle.
  *
  * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and
- * bench.py's cpu_baseline leg may load this library, and only as the checker
+ * bench.py's cpu_baseline leg may load this library, and only to check results
  * (or the timed CPU baseline); the product path never calls it.
  *
  * Every function cites the reference file:line it restates.  Pinned by
