@@ -43,6 +43,16 @@ __global__ void extent_init_kernel(unsigned long long *ext, int64_t nslots) {
         ext[i] = (i & 1) ? 0ULL : ~0ULL;  // even slots are minima, odd slots maxima
 }
 
+// Widens a halo's (min, max, shifted min, shifted max) keys.  The keys only
+// move outwards, so a plain read first skips the atomics that would change
+// nothing (most warps of a large halo), sparing the contention on its keys.
+__device__ __forceinline__ void ext_update(unsigned long long *e, const unsigned long long (&k)[4]) {
+    if (k[0] < __ldcg(e + 0)) atomicMin(e + 0, k[0]);
+    if (k[1] > __ldcg(e + 1)) atomicMax(e + 1, k[1]);
+    if (k[2] < __ldcg(e + 2)) atomicMin(e + 2, k[2]);
+    if (k[3] > __ldcg(e + 3)) atomicMax(e + 3, k[3]);
+}
+
 __global__ void extent_kernel(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
                               const double *__restrict__ z, const int32_t *__restrict__ hid,
                               double box, unsigned long long *__restrict__ ext) {
@@ -70,15 +80,9 @@ __global__ void extent_kernel(int64_t n, const double *__restrict__ x, const dou
                     k[0] = min(k[0], o0); k[1] = max(k[1], o1);
                     k[2] = min(k[2], o2); k[3] = max(k[3], o3);
                 }
-                if (lane == 0 && h0 >= 0) {
-                    unsigned long long *e = ext + (int64_t)h0 * 12 + 4 * a;
-                    atomicMin(e + 0, k[0]); atomicMax(e + 1, k[1]);
-                    atomicMin(e + 2, k[2]); atomicMax(e + 3, k[3]);
-                }
+                if (lane == 0 && h0 >= 0) ext_update(ext + (int64_t)h0 * 12 + 4 * a, k);
             } else if (valid) {
-                unsigned long long *e = ext + (int64_t)h * 12 + 4 * a;
-                atomicMin(e + 0, k[0]); atomicMax(e + 1, k[1]);
-                atomicMin(e + 2, k[2]); atomicMax(e + 3, k[3]);
+                ext_update(ext + (int64_t)h * 12 + 4 * a, k);
             }
         }
     }
