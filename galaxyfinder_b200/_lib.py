@@ -182,6 +182,7 @@ SIGNATURES = {
     "findDen": (None, [_VP, _INT, _VP, _D, _D, _D, _D, _VP, _INT, _INT, _INT]),
     "gaussian_Smoothing": (None, [_VP, _INT, _INT, _INT, _D, _F]),
     "findsphdensity": (None, [_VP, _INT, _VP, _INT, _VP]),
+    "starfindsphdensity": (None, [_VP, _INT, _VP, _INT, _VP]),
     "Self_Halo_Potent": (None, [_INT, _VP, _VP, _VP]),
     "new_Make_Tree_Near": (None, [_VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _INT]),
     "Make_Tree": (None, [_VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _F, _INT]),

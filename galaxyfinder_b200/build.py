@@ -28,7 +28,7 @@ ARCHIVE = PKG / "libgf.a"  # the same objects, for linking libgf into the refere
 TUNED = PKG / "tuned.json"  # launch parameters chosen by tune.py (-D flags)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NOFMAD = {"gf_tsc.cu", "gf_knn.cu", "gf_bound.cu", "gf_cores.cu", "gf_reftree.cu", "gf_plain64.cu", "gf_plan.cu", "gf_shells.cu",
-          "gf_rtidal.cu"}
+          "gf_rtidal.cu", "gf_starden.cu"}
 
 
 def nvcc() -> str:

@@ -55,19 +55,6 @@ __device__ __forceinline__ double exact_d2(const float4 &a, const float4 &b) {
     return dx * dx + dy * dy + dz * dz;
 }
 
-// W4 kernel, nnost.c:536-555 (float arguments, double constants)
-__device__ __forceinline__ float w4(float dist, float h) {
-    const float r = dist / h;
-    if (r < 1.) {
-        return (float)((-0.2387324) * ((2. - (double)r) * (double)r * (double)r - 1.333333) /
-                       (double)(h * h * h));
-    } else if (r < 2.) {
-        const float twomr = (float)((2. - (double)r) / (double)h);
-        return (float)(0.07957747 * (double)twomr * (double)twomr * (double)twomr);
-    }
-    return 0.f;
-}
-
 // Ascending bitonic sort of one (d, i) pair per lane.
 __device__ __forceinline__ void warp_sort(double &d, int &i) {
     const int lane = threadIdx.x & 31;

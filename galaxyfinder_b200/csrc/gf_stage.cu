@@ -723,6 +723,15 @@ int do_findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex,
 }  // namespace
 
 namespace gf {
+// The findsphdensity drop-in's lists and densities for another drop-in
+// (starfindsphdensity, gf_starden.cu).
+int findsphdensity_lists(SimpleBasicParticleType *bp, int np, long long *nearindex, int numnear,
+                         float *densph) {
+    return do_findsphdensity(bp, np, nearindex, numnear, densph);
+}
+}  // namespace gf
+
+namespace gf {
 
 // Potential of the sources (sr, smass) at the targets r (self: r == sr) on
 // the device of ctx; leaves penergy in device memory (*dout) and the FP64

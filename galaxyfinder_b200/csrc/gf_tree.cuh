@@ -5,6 +5,20 @@
 
 namespace gf {
 
+// W4 kernel, nnost.c:536-555 (float arguments, double constants); the
+// translation units that use it are compiled with --fmad=false.
+__device__ __forceinline__ float w4(float dist, float h) {
+    const float r = dist / h;
+    if (r < 1.) {
+        return (float)((-0.2387324) * ((2. - (double)r) * (double)r * (double)r - 1.333333) /
+                       (double)(h * h * h));
+    } else if (r < 2.) {
+        const float twomr = (float)((2. - (double)r) / (double)h);
+        return (float)(0.07957747 * (double)twomr * (double)twomr * (double)twomr);
+    }
+    return 0.f;
+}
+
 // Builds the octree of every halo of a batch.  pos (batch order, halo h is
 // [pstart[h], pstart[h+1])) holds recentred FP32 positions and masses.
 // theta2 fills BhNode::open_r2; q5_asbuilt reproduces ost.c:571 (m*y*x in

@@ -65,6 +65,18 @@ def findsphdensity(bp, numnear):
     return near, dens
 
 
+def starfindsphdensity(bp, numnear):
+    """nnost.c:632 — stellar density (10 nearest stars, W4 times mass) at every
+    particle and every particle's k nearest neighbours (self included)."""
+    bp = _bp(bp)
+    n = len(bp)
+    near = np.zeros((n, numnear), np.int64)
+    dens = np.zeros(n, np.float32)
+    lib().starfindsphdensity(ptr(bp), n, ptr(near), numnear, ptr(dens))
+    check_last()
+    return near, dens
+
+
 def _vec3(r) -> np.ndarray:
     r = np.asarray(r)
     if r.dtype == VEC3_DTYPE:

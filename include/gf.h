@@ -92,6 +92,11 @@ void gaussian_Smoothing(float *denGrid, int nx, int ny, int nz, double cellsize,
 /* NewGalFinder/nnost.c:560.  nearindex holds np*Numnear indices into bp. */
 void findsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, int Numnear,
                     float *densph);
+/* NewGalFinder/nnost.c:632.  densph[i]: W4-weighted mass of the 10 nearest
+ * stars (type 1) of particle i (0 when the halo has none); nearindex: the
+ * Numnear nearest particles of every particle, as findsphdensity. */
+void starfindsphdensity(SimpleBasicParticleType *bp, int np, long long *nearindex, int Numnear,
+                        float *densph);
 /* NewGalFinder/nnost.c:991.  Mesh density (TSC of the ptype particles,
  * Gaussian smoothing, findDen at every particle -> densph), the mesh peak
  * cores (*Core, *NumCore; at most maxnumcore before merging) and the kNN of

@@ -164,6 +164,7 @@ class Reference:
             L.ref_GetBGpotent.argtypes = [_D]
             L.ref_GetBGpotent.restype = _D
             L.ref_findsphdensity.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP]
+            L.ref_starfindsphdensity.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]
             L.ref_lagFindStellarCore.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _I, _VP, _VP, _I, _I,
                                                  _VP, _VP, _VP]
             L.ref_assign_density_TSC.argtypes = [_I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I, _I, _D,
@@ -206,6 +207,16 @@ class Reference:
         idx = np.zeros(n * k, np.int64)
         dens = np.zeros(n, np.float32)
         self.L.ref_findsphdensity(n, _p(x), _p(y), _p(z), _p(mass), _p(idx), k, _p(dens))
+        return idx.reshape(n, k), dens
+
+    def starfindsphdensity(self, x, y, z, mass, type_, k):
+        """nnost.c:632-744: stellar density at every particle and its k-NN list."""
+        x, y, z, mass = map(self._d, (x, y, z, mass))
+        t = np.ascontiguousarray(type_, np.int32)
+        n = len(x)
+        idx = np.zeros(n * k, np.int64)
+        dens = np.zeros(n, np.float32)
+        self.L.ref_starfindsphdensity(n, _p(t), _p(x), _p(y), _p(z), _p(mass), _p(idx), k, _p(dens))
         return idx.reshape(n, k), dens
 
     def find_near_all(self, x, y, z, mass, k):

@@ -33,6 +33,7 @@ float m_tidal[10000], r_tidal[10000]; /* NUM_MASS, header.h:97 */
 typedef struct Vector3d { double x, y, z; } Vector3d; /* subhaloden.mod6.c:70 */
 void i_potent_spline(void);                                          /* force_spline.mod3.c:81 */
 void findsphdensity(SimpleBasicParticleType *, int, long long *, int, float *); /* nnost.c:560 */
+void starfindsphdensity(SimpleBasicParticleType *, int, long long *, int, float *); /* nnost.c:632 */
 void lagFindStellarCore(SimpleBasicParticleType *, int, int, float *, Coretype **, int *, int,
                         long long *, int);                           /* nnost.c:991 */
 void assign_density_TSC(SimpleBasicParticleType *, int, float *, int, int, int, double, double,
@@ -102,6 +103,17 @@ int ref_findsphdensity(int np, const double *x, const double *y, const double *z
     if (!g_ready) return -1;
     SimpleBasicParticleType *bp = make_bp(np, NULL, x, y, z, mass);
     findsphdensity(bp, np, nearindex, k, dens);
+    Free(bp);
+    return 0;
+}
+
+/* starfindsphdensity: stellar density (10 nearest stars, mass weighted) and
+ * the neighbour lists; the particles' types select the stars. */
+int ref_starfindsphdensity(int np, const int *type, const double *x, const double *y, const double *z,
+                           const double *mass, long long *nearindex, int k, float *dens) {
+    if (!g_ready) return -1;
+    SimpleBasicParticleType *bp = make_bp(np, type, x, y, z, mass);
+    starfindsphdensity(bp, np, nearindex, k, dens);
     Free(bp);
     return 0;
 }
