@@ -337,6 +337,8 @@ int gf_tuning_value(const char *name, int64_t *value) {
                   {"GF_BH_DYN", GF_BH_DYN},           {"GF_KNNB_DYN", GF_KNNB_DYN},
                   {"GF_BH_ACC", GF_BH_ACC},           {"GF_KNNB_WIN", GF_KNNB_WIN},
                   {"GF_KNNB_MINB", GF_KNNB_MINB},     {"GF_BH_TMA", GF_BH_TMA},
+                  {"GF_KNNB_FILT", GF_KNNB_FILT},     {"GF_KNNB_HEAPF", GF_KNNB_HEAPF},
+                  {"GF_BH_LEAF4", GF_BH_LEAF4},
                   {"GF_FFT_PENCILS_64", GF_FFT_PENCILS_64},
                   {"GF_FFT_PENCILS_128", GF_FFT_PENCILS_128}, {"GF_TSC_TILE", GF_TSC_TILE}};
     if (!name || !value) return GF_EINVAL;

@@ -748,24 +748,71 @@ __device__ __forceinline__ uint64_t pack_key(float f, int id) {
 }
 __device__ __forceinline__ float key_f(uint64_t key) { return __uint_as_float((unsigned)(key >> 32)); }
 
-// Max-heap of packed keys in one lane's column (entry e at K[32 e]).
+// Max-heap of packed keys in one lane's column (entry e at K[32 e]).  With
+// GF_KNNB_HEAPF >= 1 the heap is ordered by the float part alone (one
+// 32-bit compare per step; 2 and 3 also move the hole down first, 3 admits
+// a particle by its float distance alone): among entries of equal float distance the root is then
+// any of them, which the certification already covers (an evicted or
+// rejected particle whose float distance equals a kept one's leaves the
+// query uncertified, and the exact kernel serves it).
 __device__ __forceinline__ void kheap_sift_down(uint64_t *K, int pos, int size, uint64_t key) {
+#if GF_KNNB_HEAPF >= 2
+    // the hole left at pos descends to a leaf along the larger children (one
+    // compare per level, no test against key), then key rises from there to
+    // its place below pos
+    const unsigned kf = (unsigned)(key >> 32);
+    const int top = pos;
     while (true) {
         int c = 2 * pos + 1;
         if (c >= size) break;
         uint64_t ck = K[32 * c];
         if (c + 1 < size) {
             const uint64_t rk = K[32 * (c + 1)];
-            if (rk > ck) {
+            if ((unsigned)(rk >> 32) > (unsigned)(ck >> 32)) {
                 c++;
                 ck = rk;
             }
         }
+        K[32 * pos] = ck;
+        pos = c;
+    }
+    while (pos > top) {
+        const int p = (pos - 1) >> 1;
+        const uint64_t pk = K[32 * p];
+        if ((unsigned)(pk >> 32) >= kf) break;
+        K[32 * pos] = pk;
+        pos = p;
+    }
+    K[32 * pos] = key;
+#else
+#if GF_KNNB_HEAPF
+    const unsigned kf = (unsigned)(key >> 32);
+#endif
+    while (true) {
+        int c = 2 * pos + 1;
+        if (c >= size) break;
+        uint64_t ck = K[32 * c];
+        if (c + 1 < size) {
+            const uint64_t rk = K[32 * (c + 1)];
+#if GF_KNNB_HEAPF
+            if ((unsigned)(rk >> 32) > (unsigned)(ck >> 32)) {
+#else
+            if (rk > ck) {
+#endif
+                c++;
+                ck = rk;
+            }
+        }
+#if GF_KNNB_HEAPF
+        if (kf >= (unsigned)(ck >> 32)) break;
+#else
         if (key > ck) break;
+#endif
         K[32 * pos] = ck;
         pos = c;
     }
     K[32 * pos] = key;
+#endif
 }
 
 template <bool COUNT>
@@ -917,6 +964,10 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                         if (j < l1) {
                             cpos[lane] = pos[j];
                             cid[lane] = perm[j];
+                        } else if (GF_KNNB_FILT) {
+                            // a sentinel at infinity: its float distance is
+                            // +inf, which neither passes nor lowers frej
+                            cpos[lane] = make_float4(kInfF, kInfF, kInfF, 0.f);
                         }
                         __syncwarp();
                         const int m = min(32, l1 - base);
@@ -925,6 +976,25 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                         // the bound at its start (the bound only tightens)
                         unsigned pass = 0;
                         if (me && (base >= sw1 || base + m <= sw0)) {  // none of this lane's seeds here
+#if GF_KNNB_FILT
+                            // four candidates per step with their own
+                            // rejection minima (min is exact, so the order of
+                            // the minima does not matter); entries m..m+3 of
+                            // the last step are sentinels (t + 3 <= 31)
+                            float r1 = kInfF, r2 = kInfF, r3 = kInfF;
+                            for (int t = 0; t < m; t += 4) {
+                                const float fa = f_d2_fma(Q, cpos[t]), fb = f_d2_fma(Q, cpos[t + 1]);
+                                const float fc = f_d2_fma(Q, cpos[t + 2]), fd = f_d2_fma(Q, cpos[t + 3]);
+                                const bool oa = fa <= bf, ob = fb <= bf, oc = fc <= bf, od = fd <= bf;
+                                pass |= ((unsigned)oa | ((unsigned)ob << 1) | ((unsigned)oc << 2) | ((unsigned)od << 3))
+                                        << t;
+                                frej = fminf(frej, oa ? kInfF : fa);
+                                r1 = fminf(r1, ob ? kInfF : fb);
+                                r2 = fminf(r2, oc ? kInfF : fc);
+                                r3 = fminf(r3, od ? kInfF : fd);
+                            }
+                            frej = fminf(fminf(frej, r1), fminf(r2, r3));
+#else
 #pragma unroll 4
                             for (int t = 0; t < m; t++) {
                                 const float f = f_d2_fma(Q, cpos[t]);
@@ -932,6 +1002,7 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                                 pass |= (unsigned)ok << t;
                                 frej = ok ? frej : fminf(frej, f);
                             }
+#endif
                         } else if (me) {
 #pragma unroll 4
                             for (int t = 0; t < m; t++) {
@@ -969,8 +1040,16 @@ knn_fbucket_kernel(int64_t n, int k, const float4 *__restrict__ pos, const int32
                             const int t = __ffs(pass) - 1;
                             pass &= pass - 1;
                             const float f = f_d2_fma(Q, cpos[t]);
+#if GF_KNNB_HEAPF == 3
+                            // float test: a particle at the root's float
+                            // distance stays out and leaves the query
+                            // uncertified, as a tie evicted from the heap would
+                            if (f < bf) {
+                                const uint64_t key = pack_key(f, cid[t]);
+#else
                             const uint64_t key = pack_key(f, cid[t]);
                             if (key < rk) {
+#endif
                                 frej = fminf(frej, bf);  // the evicted root
                                 kheap_sift_down(K, 0, kk, key);
                                 rk = K[0];

@@ -236,7 +236,20 @@ bh_kernel(int64_t ntarget, const float4 *__restrict__ tpos, const int32_t *__res
 #endif
                     {
                         const int l1 = links.y + links.z;
-                        for (int j = links.y; j < l1; j++) particle_term(spos[j]);
+                        int j = links.y;
+#if GF_BH_LEAF4
+                        // four loads in flight before the terms, which are
+                        // still added in particle order
+                        for (; j + 4 <= l1; j += 4) {
+                            const float4 s0 = __ldg(spos + j), s1 = __ldg(spos + j + 1);
+                            const float4 s2 = __ldg(spos + j + 2), s3 = __ldg(spos + j + 3);
+                            particle_term(s0);
+                            particle_term(s1);
+                            particle_term(s2);
+                            particle_term(s3);
+                        }
+#endif
+                        for (; j < l1; j++) particle_term(spos[j]);
                     }
                     if (COUNT) npp += links.z;
                     my = i + 1;

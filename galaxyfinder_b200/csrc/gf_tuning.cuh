@@ -52,6 +52,15 @@
 #ifndef GF_KNNB_DYN    // float-key kNN: 1 = warps take buckets from a work counter, 0 = grid-stride
 #define GF_KNNB_DYN 0
 #endif
+#ifndef GF_KNNB_FILT   // float-key kNN tile filter: 1 = four independent chains over a sentinel-padded tile
+#define GF_KNNB_FILT 0
+#endif
+#ifndef GF_KNNB_HEAPF  // float-key kNN heaps: 1 = ordered by the float part of the key only, 2 = also hole-first sift-down, 3 = also float admission test
+#define GF_KNNB_HEAPF 0
+#endif
+#ifndef GF_BH_LEAF4    // Barnes-Hut walk: 1 = opened leaves loaded four particles at a time
+#define GF_BH_LEAF4 0
+#endif
 #ifndef GF_BH_MINB
 #define GF_BH_MINB 1
 #endif
@@ -85,6 +94,9 @@ static_assert(GF_KNNB_DYN == 0 || GF_KNNB_DYN == 1, "GF_KNNB_DYN");
 static_assert(GF_KNNB_WIN == 0 || GF_KNNB_WIN == 8 || GF_KNNB_WIN == 16 || GF_KNNB_WIN == 32, "GF_KNNB_WIN");
 static_assert(GF_BH_ACC == 0 || GF_BH_ACC == 1, "GF_BH_ACC");
 static_assert(GF_BH_TMA == 0 || GF_BH_TMA == 1, "GF_BH_TMA");
+static_assert(GF_KNNB_FILT == 0 || GF_KNNB_FILT == 1, "GF_KNNB_FILT");
+static_assert(GF_KNNB_HEAPF >= 0 && GF_KNNB_HEAPF <= 3, "GF_KNNB_HEAPF");
+static_assert(GF_BH_LEAF4 == 0 || GF_BH_LEAF4 == 1, "GF_BH_LEAF4");
 static_assert(GF_FFT_PENCILS % 2 == 0 && (GF_FFT_PENCILS / 2) * 512 / 8 <= 1024, "GF_FFT_PENCILS");
 static_assert(GF_FFT_PENCILS_64 >= 32 && GF_FFT_PENCILS_64 <= 128 &&
                   (GF_FFT_PENCILS_64 & (GF_FFT_PENCILS_64 - 1)) == 0, "GF_FFT_PENCILS_64");

@@ -13,10 +13,11 @@ the GPU and the workload), which build.py turns into -D flags.
   group   parameters                                   phase
   knn     GF_KNN_ALGO x GF_KNNB_BLOCK (x GF_KNNB_ARITY), then GF_KNNB_SEEDS,
           GF_KNNB_LANECERT, GF_KNNB_DYN, GF_KNNB_WIN x GF_KNNB_MINB
-          (node window against resident blocks) and GF_KNNB_QUEUE for the
+          (node window against resident blocks), GF_KNNB_QUEUE and
+          GF_KNNB_FILT x GF_KNNB_HEAPF (tile filter, heap order) for the
           float-key kernel; for the warp-per-query
           kernel GF_KNN_CHUNK, then GF_KNN_BLOCK x register cap   knn
-  bh      GF_BH_DYN, GF_BH_ACC, GF_BH_TMA (leaf staging), GF_BH_BLOCK,
+  bh      GF_BH_DYN, GF_BH_ACC, GF_BH_TMA (leaf staging), GF_BH_LEAF4, GF_BH_BLOCK,
           then the register cap                        potential
   fft     GF_FFT_PENCILS                               smooth
   tsc     GF_TSC_TILE (0: direct global atomics)       tsc
@@ -42,7 +43,7 @@ from . import build as B
 TUNE_DIR = B.PKG / "_tune"
 DEFAULTS = {"GF_KNN_ALGO": 2, "GF_KNNB_BLOCK": 64, "GF_KNNB_ARITY": 2, "GF_KNNB_SEEDS": 64, "GF_KNNB_QUEUE": 0, "GF_KNNB_LANECERT": 0,
             "GF_KNN_BLOCK": 256, "GF_KNN_MINB": 1, "GF_KNN_CHUNK": 32,
-            "GF_BH_BLOCK": 128, "GF_BH_DYN": 0, "GF_BH_ACC": 0, "GF_BH_TMA": 0, "GF_KNNB_DYN": 0, "GF_KNNB_WIN": 32, "GF_KNNB_MINB": 1,
+            "GF_BH_BLOCK": 128, "GF_BH_DYN": 0, "GF_BH_ACC": 0, "GF_BH_TMA": 0, "GF_BH_LEAF4": 0, "GF_KNNB_FILT": 0, "GF_KNNB_HEAPF": 0, "GF_KNNB_DYN": 0, "GF_KNNB_WIN": 32, "GF_KNNB_MINB": 1,
             "GF_BH_MINB": 1, "GF_FFT_PENCILS": 32, "GF_FFT_PENCILS_64": 32, "GF_FFT_PENCILS_128": 32, "GF_TSC_TILE": 0, "GF_TREE_BLOCK": 256}
 REGCAPS = (255, 64, 48)
 
@@ -64,6 +65,8 @@ def stages(group: str):
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else
                 [{"GF_KNNB_WIN": w, "GF_KNNB_MINB": mb} for w, mb in ((32, 1), (8, 6), (0, 6), (0, 1))],
                 lambda base: [] if base["GF_KNN_ALGO"] != 2 else [{"GF_KNNB_QUEUE": q} for q in (0, 2, 4, 8)],
+                lambda base: [] if base["GF_KNN_ALGO"] != 2 else
+                [{"GF_KNNB_FILT": f, "GF_KNNB_HEAPF": h} for f in (0, 1) for h in (0, 1, 2, 3)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else [{"GF_KNN_CHUNK": c} for c in (16, 32, 64)],
                 lambda base: [] if base["GF_KNN_ALGO"] != 0 else
                 [{"GF_KNN_BLOCK": b, "GF_KNN_MINB": minb(b, r)} for b in (128, 256) for r in REGCAPS]]
@@ -71,6 +74,7 @@ def stages(group: str):
         return [lambda base: [{"GF_BH_DYN": d} for d in (0, 1)],
                 lambda base: [{"GF_BH_ACC": a} for a in (0, 1)],
                 lambda base: [{"GF_BH_TMA": t} for t in (0, 1)],
+                lambda base: [{"GF_BH_LEAF4": v} for v in (0, 1)],
                 lambda base: [{"GF_BH_BLOCK": b, "GF_BH_MINB": 1} for b in (64, 128, 256)],
                 lambda base: [{"GF_BH_MINB": minb(base["GF_BH_BLOCK"], r)} for r in REGCAPS]]
     if group == "fft":

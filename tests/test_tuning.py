@@ -19,7 +19,8 @@ def _valid(p):
     assert 128 <= p["GF_TREE_BLOCK"] <= 1024
     assert p["GF_TSC_TILE"] == 0 or 1024 <= p["GF_TSC_TILE"] <= 12288
     assert p["GF_KNNB_WIN"] in (0, 8, 16, 32)
-    assert p["GF_BH_TMA"] in (0, 1)
+    assert p["GF_BH_TMA"] in (0, 1) and p["GF_BH_LEAF4"] in (0, 1)
+    assert p["GF_KNNB_FILT"] in (0, 1) and p["GF_KNNB_HEAPF"] in (0, 1, 2, 3)
     for b, m in ((p["GF_KNN_BLOCK"], p["GF_KNN_MINB"]), (p["GF_BH_BLOCK"], p["GF_BH_MINB"]),
                  (p["GF_KNNB_BLOCK"], p["GF_KNNB_MINB"])):
         assert m >= 1 and b * m <= 2048  # resident threads per SM
@@ -46,7 +47,8 @@ def test_search_space_is_valid():
         assert len(T.stages("knn")[3](base)) == (2 if algo == 2 else 0)  # work counter or grid-stride
         assert len(T.stages("knn")[4](base)) == (4 if algo == 2 else 0)  # node window x resident blocks
         assert len(T.stages("knn")[5](base)) == (4 if algo == 2 else 0)  # survivor queues
-        assert len(T.stages("knn")[6](base)) == (3 if algo == 0 else 0)
+        assert len(T.stages("knn")[6](base)) == (8 if algo == 2 else 0)  # tile filter x heap order
+        assert len(T.stages("knn")[7](base)) == (3 if algo == 0 else 0)
 
 
 def test_tuned_params_become_flags(tmp_path, monkeypatch):
