@@ -45,12 +45,12 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # each phase's dominant kernel, from one ncu capture of the 1024-halo
 # catalogue (1,281,067 particles); the traffic scales with the particles
 # processed.
-TRAFFIC_PER_PARTICLE = {"knn": (60.081152e6 + 115.645e6) / 1281067}
+TRAFFIC_PER_PARTICLE = {"knn": (59.67e6 + 115.437e6) / 1281067}
 # What bounds the kNN kernel instead of HBM, from the same capture: the tree
 # walk is latency- and issue-bound (its HBM traffic is the neighbour lists).
-KNN_LIMITER = ("latency/issue: 68.7% of issue slots active, 36.0% of warp slots occupied (6 blocks of 4 "
+KNN_LIMITER = ("latency/issue: 68.7% of issue slots active, 35.9% of warp slots occupied (6 blocks of 4 "
                "warps per SM: 79 registers and 35.3 KB of heaps per block), dominant stall 'wait'; "
-               "DRAM 0.64% of peak")
+               "DRAM 0.69% of peak")
 
 
 def parse():
