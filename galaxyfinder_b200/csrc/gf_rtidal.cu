@@ -147,7 +147,13 @@ int gf_nfw_rtidal_cells(void) { return kCells; }
 // mkRtidal.c:80: builds the table (on the GPU of the default context) into
 // the library's host copy that nfw_rtidal reads.
 void mkRtidal(void) {
+    clear_status();
     gf_ctx *ctx = default_ctx();
+    if (!ctx) {
+        const int st = last_status() ? last_status() : GF_EDEVICE;
+        dropin_exit_on_error(st, "mkRtidal");
+        return;
+    }
     float *d = nullptr;
     int st = GF_OK;
     std::vector<float> host((size_t)kCells);

@@ -2,8 +2,10 @@
 include/gf.h declares, and the host-only planner follows the reference's
 mesh sizing rule.  No kernel is launched here."""
 import ctypes
+import os
 import re
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -33,6 +35,23 @@ def test_library_loads_and_exports_every_declared_symbol(gf):
                          capture_output=True, text=True, check=True).stdout
     exported = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
     assert set(names) <= exported
+
+
+def test_dropins_report_a_missing_device(gf):
+    """Without a GPU a drop-in fails loudly: with GF_NOEXIT set it returns and
+    leaves the status, without it the process exits with code 99 and names
+    the function (the reference's callers have no status to read)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    gf.mkRtidal()
+    assert gf.gf_last_status() != 0
+    assert gf.nfw_rtidal(0.01, 0.5, 10.0) == 0.0  # no table was built
+    code = "import ctypes, sys; ctypes.CDLL(sys.argv[1]).mkRtidal(); print('returned')"
+    env = {k: v for k, v in os.environ.items() if k != "GF_NOEXIT"}
+    r = subprocess.run([sys.executable, "-c", code, str(ROOT / "galaxyfinder_b200/libgf.so")], env=env,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 99 and "mkRtidal" in r.stderr and "returned" not in r.stdout
 
 
 def test_status_strings(gf):
