@@ -365,6 +365,30 @@ int or_sph_density(int64_t np, int k, const double *d2, float *dens) {
     return 0;
 }
 
+/* starfindsphdensity's stellar density, nnost.c:687-703: for each particle,
+ * over its k nearest stars in distance order (d2: their exact FP64 squared
+ * distances; sidx: star indices into smass, the stars' masses as float),
+ * W4(sqrtf(d2_j), r_k/2) * m_j summed in float, r_k = sqrtf of the last d2
+ * (Find_Near's maxr).  cnt[i] < k where the halo has fewer than k stars. */
+int or_star_density(int64_t np, int k, const double *d2, const int64_t *sidx, const int32_t *cnt,
+                    const float *smass, float *dens) {
+    for (int64_t i = 0; i < np; i++) {
+        const double *l = d2 + i * k;
+        const int64_t *s = sidx + i * k;
+        const int res = cnt[i];
+        float rho = 0.f;
+        if (res > 0) {
+            float neardist = sqrtf((float)l[res - 1]);
+            for (int j = 0; j < res; j++) {
+                float dj = sqrtf((float)l[j]);
+                rho += W4(dj, (float)(neardist / 2.)) * smass[s[j]];
+            }
+        }
+        dens[i] = rho;
+    }
+    return 0;
+}
+
 /* ---------------------------------------------------------------- potential */
 /* Node record exported by libgf (gf_tree_export), preorder. */
 typedef struct {

@@ -43,6 +43,8 @@ int or_knn_grid(int64_t np, const float *x, const float *y, const float *z, int 
  * rho_i = sum_j W4(sqrtf(d2_ij), sqrtf(d2_ik)/2) in the reference's float/double
  * arithmetic (W4: nnost.c:536-555). */
 int or_sph_density(int64_t np, int k, const double *d2, float *dens);
+int or_star_density(int64_t np, int k, const double *d2, const int64_t *sidx, const int32_t *cnt,
+                    const float *smass, float *dens);
 
 
 

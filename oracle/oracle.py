@@ -61,6 +61,7 @@ class Restatement:
             L.or_knn_brute.argtypes = [_I64, _VP, _VP, _VP, _I, _VP, _VP]
             L.or_knn_grid.argtypes = [_I64, _VP, _VP, _VP, _I, _VP, _VP]
             L.or_sph_density.argtypes = [_I64, _I, _VP, _VP]
+            L.or_star_density.argtypes = [_I64, _I, _VP, _VP, _VP, _VP, _VP]
             L.or_tree_potential.argtypes = [ctypes.c_int32, _VP, _I64, _VP, _VP, _VP, _VP, _I64,
                                             _VP, _VP, _VP, _VP, _VP, _VP, _VP]
             L.or_direct_potential.argtypes = [_I64, _VP, _VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP]
@@ -115,6 +116,19 @@ class Restatement:
         self.L.or_sph_density(n, k, _p(d2), _p(out))
         return out
 
+
+    def star_density(self, d2, sidx, cnt, smass):
+        """starfindsphdensity's stellar density (nnost.c:687-703) from each
+        particle's k nearest stars: d2 and sidx (n, k) in distance order, cnt
+        (n,) the stars found, smass the stars' masses."""
+        d2 = np.ascontiguousarray(d2, np.float64)
+        sidx = np.ascontiguousarray(sidx, np.int64)
+        cnt = np.ascontiguousarray(cnt, np.int32)
+        smass = np.ascontiguousarray(smass, np.float32)
+        n, k = d2.shape
+        out = np.zeros(n, np.float32)
+        self.L.or_star_density(n, k, _p(d2), _p(sidx), _p(cnt), _p(smass), _p(out))
+        return out
 
     def tree_potential(self, nodes, spos4, tpos, troot, trend, topen=None):
         """FP64 walk of an exported tree.  nodes: BH_NODE_DTYPE array;

@@ -113,8 +113,26 @@ def main():
                         bg_1e12=ref.bg_potent(1e12), bg_mass=ref.bg_potent(float(np.sum(mf, dtype=np.float64))))
     bound_fixture(ref)
     cores_fixture(ref)
+    starden_fixture(ref)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
+
+
+def starden_fixture(ref):
+    """starfindsphdensity (nnost.c:632-744): the stellar density of every
+    particle over its 10 nearest stars and every particle's 32-neighbour
+    list, for a halo with 20 % stars and one with 6 stars (fewer than 10)."""
+    out = {}
+    for tag, seed, n, frac in (("a", 41, 1500, 0.2), ("b", 42, 300, 0.02)):
+        p = blob(seed, n, 0.03).astype(np.float32).astype(np.float64)  # float-representable
+        rng = np.random.default_rng(seed + 100)
+        typ = np.full(n, 2, np.int32)
+        typ[rng.choice(n, max(1, int(round(frac * n))), replace=False)] = 1
+        mass = np.where(typ == 1, 10.0 ** rng.uniform(6, 7, n), 1e8)
+        idx, dens = ref.starfindsphdensity(p[:, 0], p[:, 1], p[:, 2], mass, typ, 32)
+        out.update({f"pos_{tag}": p, f"mass_{tag}": mass, f"type_{tag}": typ,
+                    f"idx_{tag}": idx.astype(np.int32), f"dens_{tag}": dens})
+    np.savez_compressed(OUT / "starden.npz", **out)
 
 
 def cores_fixture(ref):
